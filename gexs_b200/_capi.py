@@ -1,0 +1,117 @@
+"""ctypes binding of include/gexs_b200.h (libgexs_b200.so, built in-tree).
+
+Loading fails loudly when the library is missing: there is no fallback
+path.  Structures mirror the C layouts field by field.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgexs_b200.so")
+
+GEXS_OK = 0
+GEXS_ERR_NOT_READY = -5
+
+GAUSSIAN, DOPPLER, VOIGT, VOIGT_QUAD = 0, 1, 2, 4
+FP64, FP32 = 0, 1
+WINDOW_INCLUSIVE, WINDOW_ROUNDED = 0, 1
+ERF_STABLE, ERF_LITERAL = 0, 1
+CONV_PHYSICAL, CONV_REF_CPU, CONV_REF_GPU = 0, 1, 2
+
+
+class GexsLines(C.Structure):
+    _fields_ = [("nu", C.c_void_p), ("elow", C.c_void_p), ("aif", C.c_void_p),
+                ("gns", C.c_void_p), ("gamma", C.c_void_p), ("n", C.c_void_p),
+                ("count", C.c_int64)]
+
+
+class GexsJob(C.Structure):
+    _fields_ = [("lines", GexsLines), ("out", C.c_void_p),
+                ("nu_start", C.c_double), ("dnu", C.c_double),
+                ("grid_points", C.c_int64), ("start_idx", C.c_int64), ("n_points", C.c_int64),
+                ("profile", C.c_int32), ("precision", C.c_int32),
+                ("window_rule", C.c_int32), ("accumulate", C.c_int32),
+                ("quad_nodes", C.c_int32), ("erf_form", C.c_int32),
+                ("cutoff", C.c_double), ("partition", C.c_double), ("beta", C.c_double),
+                ("s_scale", C.c_double), ("s_scale2", C.c_double), ("dop_coef", C.c_double),
+                ("inv_width", C.c_double), ("t_ratio", C.c_double),
+                ("gamma_scale", C.c_double), ("out_scale", C.c_double)]
+
+
+class GexsLaunchCfg(C.Structure):
+    _fields_ = [("bins_per_lane", C.c_int32), ("warps", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32)]
+
+
+# (name, restype, argtypes) for every symbol of include/gexs_b200.h
+SIGNATURES = [
+    ("gexs_version", C.c_int, []),
+    ("gexs_status_string", C.c_char_p, [C.c_int]),
+    ("gexs_last_error", C.c_char_p, []),
+    ("gexs_job_init", C.c_int, [C.POINTER(GexsJob), C.c_int, C.c_int, C.c_double, C.c_double,
+                                C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_double, C.c_double, C.c_double, C.c_int64]),
+    ("gexs_ctx_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("gexs_ctx_destroy", C.c_int, [C.c_void_p]),
+    ("gexs_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gexs_run", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
+                           C.POINTER(GexsLaunchCfg), C.c_void_p]),
+    ("gexs_count_evals", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
+                                   C.POINTER(C.c_int64)]),
+    ("gexs_batch_create", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
+                                    C.POINTER(GexsLaunchCfg), C.POINTER(C.c_void_p)]),
+    ("gexs_batch_launch", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gexs_batch_capture", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gexs_batch_replay", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gexs_batch_destroy", C.c_int, [C.c_void_p]),
+    ("gexs_autotune", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
+                                C.POINTER(GexsLaunchCfg), C.POINTER(C.c_float)]),
+    ("gexs_partition", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                 C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
+    ("gexs_manager_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
+                                      C.POINTER(C.c_void_p)]),
+    ("gexs_manager_destroy", C.c_int, [C.c_void_p]),
+    ("gexs_manager_initialize_vectors", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("gexs_manager_initialize_constants", C.c_int, [C.c_void_p] + [C.c_double] * 8),
+    ("gexs_manager_transfer_freq", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    ("gexs_manager_transfer_vectors", C.c_int, [C.c_void_p, C.c_size_t] + [C.c_void_p] * 6),
+    ("gexs_manager_execute", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                       C.c_double, C.c_double, C.c_double]),
+    ("gexs_manager_transfer_results", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int, C.c_int]),
+    ("gexs_manager_ntrans", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("gexs_manager_ready", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+]
+
+_lib = None
+
+
+def lib():
+    """Load libgexs_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libgexs_b200.so is missing: run `python -m gexs_b200.build` "
+                               "(the CUDA library is required; there is no CPU fallback)")
+        h = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+class GexsError(RuntimeError):
+    def __init__(self, status, where):
+        L = lib()
+        msg = L.gexs_last_error().decode(errors="replace")
+        super().__init__("%s failed: %s (%d): %s" % (
+            where, L.gexs_status_string(status).decode(), status, msg))
+        self.status = status
+
+
+def check(status, where):
+    if status != GEXS_OK:
+        raise GexsError(status, where)
+    return status

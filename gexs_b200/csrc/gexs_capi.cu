@@ -1,0 +1,534 @@
+/*
+ * gexs_capi.cu — C ABI of the engine: contexts, one-shot runs, batches
+ * captured into CUDA graphs, the launch-shape autotuner, convention presets,
+ * eval counting and the partition function.
+ *
+ * Errors never print or exit (the reference's CheckCudaError prints and
+ * calls exit(-1), compute/CUDA/cuda_utils.cu:8-17): every entry point
+ * returns a status and leaves a message for gexs_last_error().
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "gexs_internal.h"
+
+namespace gexs {
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_error(cudaError_t e, const char* where)
+{
+    return set_error(GEXS_ERR_CUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" +
+                                        cudaGetErrorString(e) + ")");
+}
+
+int validate_job(const gexs_job& j, int i)
+{
+    auto bad = [&](const char* what) {
+        return set_error(GEXS_ERR_INVALID, "job " + std::to_string(i) + ": " + what);
+    };
+    if (profile_class(j) < 0) return bad("unsupported profile (or quad_nodes not 16/32)");
+    if (j.precision != GEXS_FP32 && j.precision != GEXS_FP64) return bad("precision");
+    if (j.window_rule != GEXS_WINDOW_INCLUSIVE && j.window_rule != GEXS_WINDOW_ROUNDED)
+        return bad("window_rule");
+    if (j.erf_form != GEXS_ERF_STABLE && j.erf_form != GEXS_ERF_LITERAL) return bad("erf_form");
+    if (!j.out) return bad("out is NULL");
+    if (j.lines.count < 0) return bad("negative line count");
+    if (j.lines.count > 0 && (!j.lines.nu || !j.lines.elow || !j.lines.aif || !j.lines.gns))
+        return bad("line arrays are NULL");
+    bool press = j.profile == GEXS_VOIGT || j.profile == GEXS_VOIGT_QUAD;
+    if (press && j.lines.count > 0 && (!j.lines.gamma || !j.lines.n))
+        return bad("gamma/n arrays required by this profile");
+    if (!(j.dnu > 0.0) || !std::isfinite(j.nu_start)) return bad("grid spacing must be > 0");
+    if (j.grid_points < 1 || j.start_idx < 0 || j.n_points < 0 ||
+        j.start_idx + j.n_points > j.grid_points)
+        return bad("sub-range outside the grid");
+    if (!(j.cutoff >= 0.0) || !std::isfinite(j.cutoff)) return bad("cutoff");
+    if (j.cutoff / j.dnu > 4.0e6) return bad("cutoff/dnu above 4e6 bins");
+    if (!(j.partition > 0.0)) return bad("partition must be > 0");
+    if (j.profile == GEXS_GAUSSIAN && !(j.inv_width > 0.0)) return bad("inv_width");
+    if (j.profile != GEXS_GAUSSIAN && !(j.dop_coef > 0.0)) return bad("dop_coef");
+    return GEXS_OK;
+}
+
+}  // namespace gexs
+
+using namespace gexs;
+
+/* ----------------------------------------------------------- context */
+struct gexs_ctx {
+    int device = 0;
+    int nsm = 148;
+    int* d_err = nullptr;            /* sticky kernel error word */
+    std::mutex mu;
+    std::map<int, gexs_launch_cfg> tuned;   /* key: pk*4 + prec */
+};
+
+static gexs_launch_cfg default_cfg(int pk, int prec)
+{
+    gexs_launch_cfg c;
+    c.bins_per_lane = 4;
+    c.warps = 8;
+    c.ctas_per_sm = 0;
+    c.reserved = 0;
+    (void)pk; (void)prec;
+    return c;
+}
+
+static bool cfg_ok(const gexs_launch_cfg& c)
+{
+    return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8) &&
+           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0;
+}
+
+static gexs_launch_cfg ctx_cfg(gexs_ctx* ctx, int pk, int prec)
+{
+    std::lock_guard<std::mutex> g(ctx->mu);
+    auto it = ctx->tuned.find(pk * 4 + prec);
+    return it == ctx->tuned.end() ? default_cfg(pk, prec) : it->second;
+}
+
+/* a group = jobs of one (profile class, precision): one kernel launch */
+struct Group {
+    int pk, prec;
+    std::vector<gexs_job> jobs;
+    std::vector<int> prefix;
+    int nitems = 0;
+};
+
+static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg_in,
+                        gexs_ctx* ctx, std::vector<Group>& groups,
+                        std::vector<gexs_launch_cfg>& cfgs)
+{
+    groups.clear(); cfgs.clear();
+    if (njobs < 0 || (njobs > 0 && !jobs)) return set_error(GEXS_ERR_INVALID, "jobs");
+    std::map<int, int> gi;
+    for (int i = 0; i < njobs; ++i) {
+        int st = validate_job(jobs[i], i);
+        if (st) return st;
+        int pk = profile_class(jobs[i]), prec = jobs[i].precision;
+        int key = pk * 4 + prec;
+        if (!gi.count(key)) {
+            gi[key] = (int)groups.size();
+            Group g; g.pk = pk; g.prec = prec; g.prefix.push_back(0);
+            groups.push_back(g);
+            gexs_launch_cfg c = cfg_in ? *cfg_in : ctx_cfg(ctx, pk, prec);
+            if (!cfg_ok(c)) return set_error(GEXS_ERR_INVALID, "launch configuration");
+            cfgs.push_back(c);
+        }
+        Group& g = groups[gi[key]];
+        int W = tile_bins(cfgs[gi[key]]);
+        int64_t tiles = (jobs[i].n_points + W - 1) / W;
+        if ((int64_t)g.nitems + tiles > (int64_t)INT32_MAX)
+            return set_error(GEXS_ERR_INVALID, "too many tiles in one launch");
+        g.jobs.push_back(jobs[i]);
+        g.nitems += (int)tiles;
+        g.prefix.push_back(g.nitems);
+    }
+    return GEXS_OK;
+}
+
+/* device image of a group: [jobs][prefix][counter] */
+static size_t group_bytes(const Group& g, size_t* off_prefix, size_t* off_counter)
+{
+    size_t a = g.jobs.size() * sizeof(gexs_job);
+    a = (a + 255) & ~size_t(255);
+    *off_prefix = a;
+    a += g.prefix.size() * sizeof(int);
+    a = (a + 255) & ~size_t(255);
+    *off_counter = a;
+    return a + 256;
+}
+
+static std::vector<unsigned char> group_image(const Group& g, size_t bytes, size_t op, size_t oc)
+{
+    std::vector<unsigned char> h(bytes, 0);
+    std::memcpy(h.data(), g.jobs.data(), g.jobs.size() * sizeof(gexs_job));
+    std::memcpy(h.data() + op, g.prefix.data(), g.prefix.size() * sizeof(int));
+    (void)oc;
+    return h;
+}
+
+extern "C" {
+
+int gexs_version(void) { return 100; }
+
+const char* gexs_status_string(int s)
+{
+    switch (s) {
+    case GEXS_OK: return "ok";
+    case GEXS_ERR_INVALID: return "invalid argument";
+    case GEXS_ERR_OOM: return "out of memory";
+    case GEXS_ERR_CUDA: return "CUDA error";
+    case GEXS_ERR_TIMEOUT: return "timeout";
+    case GEXS_ERR_NOT_READY: return "not ready";
+    case GEXS_ERR_ADMISSION: return "exceeds memory budget";
+    case GEXS_ERR_SHUTDOWN: return "shutting down";
+    case GEXS_ERR_KERNEL: return "kernel error flag set";
+    }
+    return "unknown status";
+}
+
+const char* gexs_last_error(void) { return g_last_error.c_str(); }
+
+int gexs_job_init(gexs_job* job, int convention, int profile, double temperature,
+                  double pressure, double partition, double mean_mass, double ref_temp,
+                  double ref_press, double half_width, double cutoff, double nu_start,
+                  double dnu, int64_t grid_points)
+{
+    if (!job) return set_error(GEXS_ERR_INVALID, "job is NULL");
+    if (!(temperature > 0.0) || !(mean_mass > 0.0 || profile == GEXS_GAUSSIAN))
+        return set_error(GEXS_ERR_INVALID, "temperature and mass must be > 0");
+    if (!(dnu > 0.0) || grid_points < 1) return set_error(GEXS_ERR_INVALID, "grid");
+    gexs_job j;
+    std::memset(&j, 0, sizeof(j));
+    j.profile = profile;
+    j.precision = GEXS_FP64;
+    j.quad_nodes = 16;
+    j.nu_start = nu_start; j.dnu = dnu; j.grid_points = grid_points;
+    j.start_idx = 0; j.n_points = grid_points;
+    j.partition = partition;
+    j.s_scale2 = 1.0;
+    j.gamma_scale = 1.0;
+    j.t_ratio = ref_temp / temperature;
+    /* cgs constants of common/defines.h:23-25 */
+    const double PLANCK = 6.6260693e-27, VELLGT = 2.99792458e+10, BOLTZ = 1.380658e-16;
+    const bool press = profile == GEXS_VOIGT || profile == GEXS_VOIGT_QUAD;
+    if (convention == GEXS_CONV_PHYSICAL) {
+        const double NA = 6.02214129e+23;                 /* GPUManager.cpp:34 */
+        const double pi = std::acos(-1.0);
+        j.beta = PLANCK * VELLGT / (BOLTZ * temperature);
+        j.s_scale = 1.0 / (8.0 * pi * VELLGT);
+        j.dop_coef = std::sqrt(2.0 * BOLTZ * temperature * NA / mean_mass) / VELLGT;
+        if (profile == GEXS_GAUSSIAN) j.inv_width = std::sqrt(std::log(2.0)) / half_width;
+        j.gamma_scale = pressure / 1.01325;               /* bar -> atm */
+        j.cutoff = cutoff >= 0.0 ? cutoff : 25.0;
+        j.window_rule = GEXS_WINDOW_INCLUSIVE;
+        j.erf_form = GEXS_ERF_STABLE;
+        j.out_scale = press ? 1.0 / std::sqrt(pi) : 0.5 / dnu;
+    } else if (convention == GEXS_CONV_REF_CPU) {
+        /* Managers/CPU/OpenMPManager.cpp: constants of common/defines.h */
+        const double PI = 3.14159265359, LN2 = 0.69314718056, NA = 6.0221412927e23;
+        const double ISQRTPI = 0.564189584;
+        j.beta = PLANCK * VELLGT / (BOLTZ * temperature);
+        j.s_scale = 1.0 / (8.0 * PI * VELLGT);             /* :115 */
+        j.s_scale2 = press ? ISQRTPI : 1.0;                 /* :394 vs :296 */
+        j.dop_coef = std::sqrt(2.0 * LN2 * BOLTZ * temperature * NA / (mean_mass)) / VELLGT;
+        if (profile == GEXS_GAUSSIAN) j.inv_width = 0.832554611 / half_width;
+        j.gamma_scale = 1.0;                                /* :398, no pressure */
+        if (cutoff >= 0.0) j.cutoff = cutoff;
+        else if (press) j.cutoff = std::min(25.0 * pressure, 100.0);   /* :386 */
+        else if (profile == GEXS_GAUSSIAN) j.cutoff = 10.0 * half_width;
+        else j.cutoff = 100.0;                              /* DOPPLER_CUTOFF */
+        j.window_rule = GEXS_WINDOW_ROUNDED;
+        j.erf_form = GEXS_ERF_LITERAL;
+        j.out_scale = (profile == GEXS_GAUSSIAN) ? 0.5 / dnu : 1.0;
+    } else if (convention == GEXS_CONV_REF_GPU) {
+        /* compute/CUDA/cross_kernal_v2.cu with GPUManager.cpp:29-49 */
+        const double SQRTLN2 = 0.832554611, ISQRTPI = 0.564189584, CM_COEF = 1.327209365e-12;
+        const double avogno = 6.02214129e+23, ln2 = std::log(2.0);
+        const double dpwco = std::sqrt(2.0 * ln2 * BOLTZ * avogno / mean_mass) / VELLGT;
+        j.beta = PLANCK * VELLGT / (BOLTZ * temperature);
+        j.s_scale = CM_COEF;
+        j.dop_coef = std::sqrt(temperature) * dpwco / SQRTLN2;
+        if (profile == GEXS_GAUSSIAN) j.inv_width = SQRTLN2 / half_width;
+        j.gamma_scale = pressure * ref_press;               /* :142 */
+        if (cutoff >= 0.0) j.cutoff = cutoff;
+        else if (profile == GEXS_GAUSSIAN) j.cutoff = 10.0 * half_width;
+        else j.cutoff = 100.0;                              /* LORENTZ/DOPPLER_CUTOFF */
+        j.window_rule = GEXS_WINDOW_INCLUSIVE;
+        j.erf_form = GEXS_ERF_LITERAL;
+        j.out_scale = press ? ISQRTPI : 0.5 / dnu;
+    } else {
+        return set_error(GEXS_ERR_INVALID, "unknown convention");
+    }
+    *job = j;
+    return GEXS_OK;
+}
+
+int gexs_ctx_create(int device, gexs_ctx** out)
+{
+    if (!out) return set_error(GEXS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    gexs_ctx* c = new gexs_ctx();
+    c->device = device;
+    e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) { delete c; return cuda_error(e, "cudaDeviceGetAttribute"); }
+    e = cudaMalloc(&c->d_err, sizeof(int));
+    if (e != cudaSuccess) { delete c; return set_error(GEXS_ERR_OOM, "error word"); }
+    cudaMemset(c->d_err, 0, sizeof(int));
+    *out = c;
+    return GEXS_OK;
+}
+
+int gexs_ctx_destroy(gexs_ctx* ctx)
+{
+    if (!ctx) return GEXS_OK;
+    cudaSetDevice(ctx->device);
+    cudaFree(ctx->d_err);
+    delete ctx;
+    return GEXS_OK;
+}
+
+int gexs_ctx_check(gexs_ctx* ctx, void* stream)
+{
+    if (!ctx) return set_error(GEXS_ERR_INVALID, "ctx is NULL");
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
+    int flag = 0;
+    e = cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "read error word");
+    if (flag) return set_error(GEXS_ERR_KERNEL, "kernel error flag " + std::to_string(flag));
+    return GEXS_OK;
+}
+
+int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
+             void* stream)
+{
+    if (!ctx) return set_error(GEXS_ERR_INVALID, "ctx is NULL");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    std::vector<Group> groups;
+    std::vector<gexs_launch_cfg> cfgs;
+    int st = build_groups(jobs, njobs, cfg, ctx, groups, cfgs);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        if (g.nitems == 0) continue;
+        size_t op, oc;
+        size_t bytes = group_bytes(g, &op, &oc);
+        std::vector<unsigned char> h = group_image(g, bytes, op, oc);
+        void* d = nullptr;
+        e = cudaMallocAsync(&d, bytes, s);
+        if (e != cudaSuccess) return set_error(GEXS_ERR_OOM, "launch tables");
+        e = cudaMemcpyAsync(d, h.data(), bytes, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) { cudaFreeAsync(d, s); return cuda_error(e, "upload launch tables"); }
+        unsigned char* b = (unsigned char*)d;
+        e = launch_tiles(g.pk, g.prec, (const gexs_job*)b, (const int*)(b + op), (int)g.jobs.size(),
+                         g.nitems, (int*)(b + oc), ctx->d_err, cfgs[gi], ctx->nsm, s);
+        cudaFreeAsync(d, s);
+        if (e != cudaSuccess) return cuda_error(e, "tile kernel launch");
+    }
+    return GEXS_OK;
+}
+
+int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs, int64_t* h_counts)
+{
+    if (!ctx || !jobs || njobs <= 0 || !h_counts) return set_error(GEXS_ERR_INVALID, "arguments");
+    for (int i = 0; i < njobs; ++i) {
+        int st = validate_job(jobs[i], i);
+        if (st) return st;
+    }
+    cudaSetDevice(ctx->device);
+    gexs_job* dj = nullptr; unsigned long long* dc = nullptr;
+    cudaError_t e = cudaMalloc(&dj, sizeof(gexs_job) * njobs);
+    if (e != cudaSuccess) return set_error(GEXS_ERR_OOM, "count tables");
+    e = cudaMalloc(&dc, sizeof(unsigned long long) * njobs);
+    if (e != cudaSuccess) { cudaFree(dj); return set_error(GEXS_ERR_OOM, "count tables"); }
+    cudaMemcpy(dj, jobs, sizeof(gexs_job) * njobs, cudaMemcpyHostToDevice);
+    cudaMemset(dc, 0, sizeof(unsigned long long) * njobs);
+    e = launch_count(dj, njobs, dc, ctx->nsm, 0);
+    std::vector<unsigned long long> hc(njobs);
+    if (e == cudaSuccess) e = cudaMemcpy(hc.data(), dc, sizeof(unsigned long long) * njobs, cudaMemcpyDeviceToHost);
+    cudaFree(dj); cudaFree(dc);
+    if (e != cudaSuccess) return cuda_error(e, "count kernel");
+    for (int i = 0; i < njobs; ++i) h_counts[i] = (int64_t)hc[i];
+    return GEXS_OK;
+}
+
+}  // extern "C"
+
+/* ------------------------------------------------------------ batches */
+struct gexs_batch {
+    gexs_ctx* ctx = nullptr;
+    std::vector<Group> groups;
+    std::vector<gexs_launch_cfg> cfgs;
+    std::vector<void*> dmem;          /* per group device image */
+    std::vector<size_t> op, oc;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static int batch_enqueue(gexs_batch* b, cudaStream_t s)
+{
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const Group& g = b->groups[gi];
+        if (g.nitems == 0) continue;
+        unsigned char* d = (unsigned char*)b->dmem[gi];
+        cudaError_t e = cudaMemsetAsync(d + b->oc[gi], 0, sizeof(int), s);
+        if (e != cudaSuccess) return cuda_error(e, "reset work counter");
+        e = launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + b->op[gi]),
+                         (int)g.jobs.size(), g.nitems, (int*)(d + b->oc[gi]), b->ctx->d_err,
+                         b->cfgs[gi], b->ctx->nsm, s);
+        if (e != cudaSuccess) return cuda_error(e, "tile kernel launch");
+    }
+    return GEXS_OK;
+}
+
+extern "C" {
+
+int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+                      const gexs_launch_cfg* cfg, gexs_batch** out)
+{
+    if (!ctx || !out) return set_error(GEXS_ERR_INVALID, "arguments");
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    gexs_batch* b = new gexs_batch();
+    b->ctx = ctx;
+    int st = build_groups(jobs, njobs, cfg, ctx, b->groups, b->cfgs);
+    if (st) { delete b; return st; }
+    for (const Group& g : b->groups) {
+        size_t op, oc;
+        size_t bytes = group_bytes(g, &op, &oc);
+        std::vector<unsigned char> h = group_image(g, bytes, op, oc);
+        void* d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) { gexs_batch_destroy(b); return set_error(GEXS_ERR_OOM, "batch tables"); }
+        b->dmem.push_back(d); b->op.push_back(op); b->oc.push_back(oc);
+        cudaError_t e = cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { gexs_batch_destroy(b); return cuda_error(e, "upload batch tables"); }
+    }
+    *out = b;
+    return GEXS_OK;
+}
+
+int gexs_batch_launch(gexs_batch* b, void* stream)
+{
+    if (!b) return set_error(GEXS_ERR_INVALID, "batch is NULL");
+    cudaSetDevice(b->ctx->device);
+    return batch_enqueue(b, (cudaStream_t)stream);
+}
+
+int gexs_batch_capture(gexs_batch* b, void* stream)
+{
+    if (!b) return set_error(GEXS_ERR_INVALID, "batch is NULL");
+    cudaSetDevice(b->ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!s) return set_error(GEXS_ERR_INVALID, "capture needs a non-default stream");
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamBeginCapture");
+    int st = batch_enqueue(b, s);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+    return GEXS_OK;
+}
+
+int gexs_batch_replay(gexs_batch* b, void* stream)
+{
+    if (!b || !b->exec) return set_error(GEXS_ERR_INVALID, "batch has no captured graph");
+    cudaSetDevice(b->ctx->device);
+    cudaError_t e = cudaGraphLaunch(b->exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGraphLaunch");
+    return GEXS_OK;
+}
+
+int gexs_batch_destroy(gexs_batch* b)
+{
+    if (!b) return GEXS_OK;
+    cudaSetDevice(b->ctx->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (void* d : b->dmem) cudaFree(d);
+    delete b;
+    return GEXS_OK;
+}
+
+int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cfg* best,
+                  float* h_ms)
+{
+    if (!ctx || !jobs || njobs <= 0 || !best) return set_error(GEXS_ERR_INVALID, "arguments");
+    cudaSetDevice(ctx->device);
+    int pk = profile_class(jobs[0]), prec = jobs[0].precision;
+    for (int i = 0; i < njobs; ++i)
+        if (profile_class(jobs[i]) != pk || jobs[i].precision != prec)
+            return set_error(GEXS_ERR_INVALID, "autotune needs jobs of one profile and precision");
+    std::vector<gexs_job> tj(jobs, jobs + njobs);
+    for (auto& j : tj) j.accumulate = 0;          /* tuning runs overwrite outputs */
+    const int bins[3] = {2, 4, 8}, warps[2] = {4, 8};
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+        return set_error(GEXS_ERR_CUDA, "stream");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    float best_ms = 1e30f; gexs_launch_cfg bc = default_cfg(pk, prec);
+    int st = GEXS_OK;
+    for (int bi = 0; bi < 3 && !st; ++bi)
+        for (int wi = 0; wi < 2 && !st; ++wi) {
+            gexs_launch_cfg c; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
+            c.ctas_per_sm = 0; c.reserved = 0;
+            gexs_batch* b = nullptr;
+            st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);
+            if (st) break;
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && !st; ++rep) {
+                cudaEventRecord(e0, s);
+                st = gexs_batch_launch(b, s);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) st = set_error(GEXS_ERR_CUDA, "autotune run");
+                float t = 0.f; cudaEventElapsedTime(&t, e0, e1);
+                if (rep > 0) ms = std::min(ms, t);        /* first run warms up */
+            }
+            gexs_batch_destroy(b);
+            if (!st && ms < best_ms) { best_ms = ms; bc = c; }
+        }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (st) return st;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        ctx->tuned[pk * 4 + prec] = bc;
+    }
+    *best = bc;
+    if (h_ms) *h_ms = best_ms;
+    return GEXS_OK;
+}
+
+int gexs_partition(gexs_ctx* ctx, const double* d_energy, const int32_t* d_g, int64_t nstates,
+                   const double* h_temps, int nt, double* h_q)
+{
+    if (!ctx || !d_energy || !d_g || nstates <= 0 || !h_temps || nt <= 0 || !h_q)
+        return set_error(GEXS_ERR_INVALID, "arguments");
+    cudaSetDevice(ctx->device);
+    const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+    std::vector<double> betas(nt);
+    for (int i = 0; i < nt; ++i) {
+        if (!(h_temps[i] > 0.0)) return set_error(GEXS_ERR_INVALID, "temperature must be > 0");
+        betas[i] = planck * vellgt / (boltz * h_temps[i]);
+    }
+    int nchunk = (int)std::min<int64_t>(ctx->nsm * 2, (nstates + 255) / 256);
+    double *db = nullptr, *dp = nullptr, *dq = nullptr;
+    if (cudaMalloc(&db, sizeof(double) * nt) != cudaSuccess ||
+        cudaMalloc(&dp, sizeof(double) * (size_t)nt * nchunk) != cudaSuccess ||
+        cudaMalloc(&dq, sizeof(double) * nt) != cudaSuccess) {
+        cudaFree(db); cudaFree(dp); cudaFree(dq);
+        return set_error(GEXS_ERR_OOM, "partition buffers");
+    }
+    cudaMemcpy(db, betas.data(), sizeof(double) * nt, cudaMemcpyHostToDevice);
+    cudaError_t e = launch_partition(d_energy, d_g, nstates, db, nt, dp, nchunk, dq, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(h_q, dq, sizeof(double) * nt, cudaMemcpyDeviceToHost);
+    cudaFree(db); cudaFree(dp); cudaFree(dq);
+    if (e != cudaSuccess) return cuda_error(e, "partition kernel");
+    return GEXS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+/* gexs_internal.h — declarations shared by the library's translation units. */
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/gexs_b200.h"
+
+namespace gexs {
+
+/* kernel launchers (gexs_kernels.cu) */
+int profile_class(const gexs_job& j);
+int tile_bins(const gexs_launch_cfg& c);
+cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
+                         int njobs, int nitems, int* d_counter, int* d_err,
+                         const gexs_launch_cfg& cfg, int nsm, cudaStream_t st);
+cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,
+                         int nsm, cudaStream_t st);
+cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,
+                             const double* d_betas, int nt, double* d_partial, int nchunk,
+                             double* d_q, cudaStream_t st);
+
+/* error reporting (gexs_capi.cu): thread-local message, returns status */
+int set_error(int status, const std::string& msg);
+int cuda_error(cudaError_t e, const char* where);
+
+/* validation shared by the run paths */
+int validate_job(const gexs_job& j, int index);
+
+}  // namespace gexs

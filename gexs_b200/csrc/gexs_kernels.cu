@@ -1,0 +1,700 @@
+/*
+ * gexs_kernels.cu — sm_100a kernels of the cross-section path.
+ *
+ * Work decomposition (replaces the reference's one-CTA-per-grid-point scan
+ * over every line of a chunk, compute/CUDA/cross_kernal_v2.cu:403-457):
+ *  - a work item is one tile of W = 32*B*WARPS consecutive bins of one job;
+ *  - a persistent grid pulls items from a global counter;
+ *  - the CTA finds the lines whose window can reach its tile with two
+ *    warp-cooperative binary searches over the nu-sorted line list;
+ *  - line records stream global -> shared memory through cp.async,
+ *    double-buffered, WARPS*32 lines per stage;
+ *  - each thread derives one line per stage in FP64: S(T) (Boltzmann and
+ *    stimulated-emission factors), the Doppler width, gammaL, and the exact
+ *    integer bin limits of the line's window and of its Humlicek regions
+ *    inside the tile, computed with the same FP64 predicates as the
+ *    reference CPU path, so FP32 evaluation never changes a window or a
+ *    region decision;
+ *  - lane l of warp w owns bins wb + l + 32k (k < B) in registers and loops
+ *    over the stage's lines: no atomics, every bin sums its lines in
+ *    ascending line order (deterministic, independent of other jobs);
+ *  - FP32 form: per-stage FP32 partial sums merged into a Kahan-compensated
+ *    (sum, compensation) pair per bin; FP64 form: plain FP64 sums.
+ */
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include "gexs_device.cuh"
+#include "gexs_internal.h"
+
+namespace gexs {
+
+/* --------------------------------------------------------------- records */
+struct RecF32 {            /* 48 bytes */
+    float icf;             /* tile-relative centre bin floor(tc), exact      */
+    float dx;              /* dnu * invw                                     */
+    float mfcdx;           /* -(tc - floor(tc)) * dx                         */
+    float a1;              /* Voigt: amp*0.5641896*y ; GH: amp*y/pi          */
+    float p;               /* Voigt: 0.5 + y^2 ; GH: y^2                     */
+    float y;               /* Voigt/GH: y ; Doppler: half bin in x units     */
+    float amp;             /* Voigt/GH: S*invw*out_scale ; Doppler: S*out    */
+    float pad;
+    int   win;             /* a | b << 16 : bins [a, b) of the tile          */
+    int   c1;              /* Voigt: bins not in region I ; Doppler: bins
+                              whose xm <= zero threshold                     */
+    int   c2;              /* Voigt: bins in regions III/IV                  */
+    int   c3;              /* Voigt: bins satisfying the region-III test     */
+};
+
+struct RecF64 {            /* 48 bytes */
+    double nu;             /* centre after the nu==0 rule                   */
+    double invw;
+    double y;              /* Voigt/GH: y ; Doppler: unused                 */
+    double amp;            /* Voigt/GH: S*invw*out_scale ; Doppler: S*out   */
+    int    win, c1, c2, c3;
+};
+
+template <int PREC> struct RecOf;
+template <> struct RecOf<GEXS_FP32> { typedef RecF32 T; };
+template <> struct RecOf<GEXS_FP64> { typedef RecF64 T; };
+
+__device__ __forceinline__ int pack2(int a, int b) { return a | (b << 16); }
+__device__ __forceinline__ int lo16(int v) { return v & 0xffff; }
+__device__ __forceinline__ int hi16(int v) { return (int)((unsigned)v >> 16); }
+
+/* profile classes of the kernel template */
+enum { PK_VOIGT = 0, PK_ERF = 1, PK_GH16 = 2, PK_GH32 = 3 };
+
+/* ------------------------------------------------------- cp.async helpers */
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
+
+/* ------------------------------------------------- warp binary searches */
+/* first index in [0, n) with a[i] >= v (LE=false) or a[i] > v (LE=true) */
+template <bool LE>
+__device__ int64_t warp_bound(const double* __restrict__ a, int64_t n, double v, int lane)
+{
+    int64_t lo = 0, hi = n;
+    while (hi - lo > 32) {
+        int64_t step = (hi - lo) / 33;
+        int64_t idx = lo + step * (lane + 1);
+        double av = __ldg(a + idx);
+        bool below = LE ? (av <= v) : (av < v);
+        int c = __popc(__ballot_sync(0xffffffffu, below));
+        int64_t nlo = (c == 0) ? lo : lo + step * c + 1;
+        int64_t nhi = (c == 32) ? hi : lo + step * (c + 1);
+        lo = nlo; hi = nhi;
+    }
+    int64_t idx = lo + lane;
+    bool below = false;
+    if (idx < hi) { double av = __ldg(a + idx); below = LE ? (av <= v) : (av < v); }
+    return lo + __popc(__ballot_sync(0xffffffffu, below));
+}
+
+/* ---------------------------------------------------------- tile geometry */
+struct Tile {
+    const gexs_job* J;
+    int64_t j0;          /* absolute first bin                       */
+    int     jn;          /* bins in this tile                        */
+    double  f0, fl;      /* frequencies of first / last bin          */
+};
+
+/* window of a line inside the tile as [a, b) (tile-relative) */
+__device__ __forceinline__ void tile_window(const Tile& T, double nu, double tc,
+                                            int* pa, int* pb)
+{
+    const gexs_job& J = *T.J;
+    if (J.window_rule == GEXS_WINDOW_ROUNDED) {
+        double ib = round(ddiv(dsub(dsub(nu, J.cutoff), J.nu_start), J.dnu));
+        double ie = round(ddiv(dsub(dadd(nu, J.cutoff), J.nu_start), J.dnu));
+        double s0 = (double)J.start_idx, s1 = (double)(J.start_idx + J.n_points);
+        ib = fmax(ib, s0); ie = fmin(ie, s1);
+        double a = ib - (double)T.j0, b = ie - (double)T.j0;
+        a = fmin(fmax(a, 0.0), (double)T.jn);
+        b = fmin(fmax(b, 0.0), (double)T.jn);
+        if (b < a) b = a;
+        *pa = (int)a; *pb = (int)b;
+        return;
+    }
+    /* inclusive rule: {t : |f_t - nu| <= cut} */
+    const double cut = J.cutoff;
+    auto in = [&](int t) {
+        return fabs(dsub(grid_f(J.nu_start, J.dnu, T.j0 + t), nu)) <= cut;
+    };
+    double dmin = nu < T.f0 ? T.f0 - nu : (nu > T.fl ? nu - T.fl : 0.0);
+    if (dmin > cut * (1.0 + 1e-12) + 1e-300) { *pa = *pb = 0; return; }
+    if (in(0) && in(T.jn - 1)) { *pa = 0; *pb = T.jn; return; }
+    int tcen = (int)fmin(fmax(rint(tc), 0.0), (double)(T.jn - 1));
+    int anchor = -1;
+    if (in(tcen)) anchor = tcen;
+    else if (tcen > 0 && in(tcen - 1)) anchor = tcen - 1;
+    else if (tcen + 1 < T.jn && in(tcen + 1)) anchor = tcen + 1;
+    if (anchor < 0) { *pa = *pb = 0; return; }
+    double w = cut / J.dnu;
+    int gl = (int)fmin(fmax(ceil(tc - w), 0.0), (double)anchor);
+    int gr = (int)fmin(fmax(floor(tc + w) + 1.0, (double)anchor), (double)T.jn);
+    *pa = first_true(0, anchor, gl, [&](int t) { return in(t); });
+    *pb = first_true(anchor, T.jn, gr, [&](int t) { return !in(t); });
+}
+
+/* bins of [wa, wb) (a sub-range of the tile) where dist-predicate `in`
+ * holds; `in` must be true on one contiguous interval around the line
+ * centre.  d_thr is an estimate of the distance limit for the guesses. */
+template <typename P>
+__device__ __forceinline__ int centered(const Tile& T, int wa, int wb, double nu, double tc,
+                                        double d_thr, const P& in)
+{
+    if (wa >= wb || !(d_thr >= 0.0)) return 0;
+    double fa = grid_f(T.J->nu_start, T.J->dnu, T.j0 + wa);
+    double fb = grid_f(T.J->nu_start, T.J->dnu, T.j0 + wb - 1);
+    double dmin = nu < fa ? fa - nu : (nu > fb ? nu - fb : 0.0);
+    if (dmin > d_thr * (1.0 + 1e-9) + 1e-300) return 0;
+    int tcen = (int)fmin(fmax(rint(tc), (double)wa), (double)(wb - 1));
+    int anchor = -1;
+    if (in(tcen)) anchor = tcen;
+    else if (tcen > wa && in(tcen - 1)) anchor = tcen - 1;
+    else if (tcen + 1 < wb && in(tcen + 1)) anchor = tcen + 1;
+    if (anchor < 0) return 0;
+    double w = d_thr / T.J->dnu;
+    int gl = (int)fmin(fmax(ceil(tc - w), (double)wa), (double)anchor);
+    int gr = (int)fmin(fmax(floor(tc + w) + 1.0, (double)anchor), (double)wb);
+    int a = first_true(wa, anchor, gl, [&](int t) { return in(t); });
+    int b = first_true(anchor, wb, gr, [&](int t) { return !in(t); });
+    return pack2(a, b);
+}
+
+/* ------------------------------------------------------------ derive one line */
+struct RawLine { double nu, elow, aif, gam, nexp; int g; };
+
+template <int PK>
+struct Derived {
+    double nu, S, invw, y, tc;
+    int win, c1, c2, c3;
+};
+
+template <int PK>
+__device__ __forceinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L, double zthr)
+{
+    const gexs_job& J = *T.J;
+    Derived<PK> d;
+    double nu = L.nu == 0.0 ? 1e-6 : L.nu;
+    double t = dmul(J.s_scale, L.aif);
+    t = dmul(t, (double)L.g);
+    t = dmul(t, J.s_scale2);
+    t = dmul(t, exp(dmul(-J.beta, L.elow)));
+    t = dmul(t, dsub(1.0, exp(dmul(-J.beta, nu))));
+    double den = dmul(dmul(nu, nu), J.partition);
+    d.nu = nu;
+    d.S = ddiv(t, den);
+    d.invw = (J.profile == GEXS_GAUSSIAN) ? J.inv_width : ddiv(1.0, dmul(nu, J.dop_coef));
+    if constexpr (PK != PK_ERF) {
+        double gl = dmul(L.gam, pow(J.t_ratio, L.nexp));
+        gl = dmul(gl, J.gamma_scale);
+        d.y = dmul(gl, d.invw);
+    } else {
+        d.y = 0.0;
+    }
+    d.tc = ddiv(dsub(nu, T.f0), J.dnu);
+    int a, b;
+    tile_window(T, nu, d.tc, &a, &b);
+    d.win = pack2(a, b);
+    d.c1 = d.c2 = d.c3 = 0;
+    if (a >= b || d.S == 0.0) { d.win = 0; return d; }
+    const double invw = d.invw, y = d.y, nu_s = J.nu_start, dnu = J.dnu;
+    const int64_t j0 = T.j0;
+    auto xof = [&](int tt) { return dmul(fabs(dsub(grid_f(nu_s, dnu, j0 + tt), nu)), invw); };
+    if constexpr (PK == PK_VOIGT) {
+        /* region tests of compute/CPU/profiles.cpp:17,24,31 */
+        d.c1 = centered(T, a, b, nu, d.tc, (15.0 - y) / invw,
+                        [&](int tt) { return dadd(xof(tt), y) < 15.0; });
+        if (lo16(d.c1) < hi16(d.c1)) {
+            d.c2 = centered(T, lo16(d.c1), hi16(d.c1), nu, d.tc, (5.5 - y) / invw,
+                            [&](int tt) { return dadd(xof(tt), y) < 5.5; });
+            if (lo16(d.c2) < hi16(d.c2))
+                d.c3 = centered(T, lo16(d.c2), hi16(d.c2), nu, d.tc, ((y + 0.176) / 0.195) / invw,
+                                [&](int tt) { return y >= dsub(dmul(0.195, xof(tt)), 0.176); });
+        }
+    } else if constexpr (PK == PK_ERF) {
+        /* bins whose lower erf argument is <= zthr; beyond it both erfc
+         * terms underflow to exactly zero */
+        const double h = 0.5 * dnu;
+        d.c1 = centered(T, a, b, nu, d.tc, zthr / invw + h,
+                        [&](int tt) {
+                            double dist = fabs(dsub(grid_f(nu_s, dnu, j0 + tt), nu));
+                            return dmul(invw, dsub(dist, h)) <= zthr;
+                        });
+    }
+    return d;
+}
+
+/* ------------------------------------------------------------ kernel args */
+struct KArgs {
+    const gexs_job* jobs;
+    const int*      prefix;    /* njobs+1 tile prefix sums               */
+    int             njobs;
+    int             nitems;
+    int*            counter;   /* work counter (zeroed before launch)    */
+    int*            err;       /* sticky error word                      */
+};
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v)
+{
+    float yv = v - c;
+    float t = s + yv;
+    c = (t - s) - yv;
+    s = t;
+}
+
+/* --------------------------------------------------------- record builders */
+template <int PK>
+__device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const gexs_job& J)
+{
+    double ic = floor(d.tc);
+    ic = fmin(fmax(ic, -8388608.0), 8388607.0);
+    double dx = dmul(J.dnu, d.invw);
+    float fc = (float)(d.tc - ic);
+    q.icf = (float)ic;
+    q.dx = (float)dx;
+    q.mfcdx = -fc * q.dx;
+    double ampd = (PK == PK_ERF) ? dmul(d.S, J.out_scale) : dmul(dmul(d.S, d.invw), J.out_scale);
+    q.amp = (float)ampd;
+    if constexpr (PK == PK_VOIGT) {
+        q.a1 = (float)(ampd * 0.5641896 * d.y);
+        q.p = (float)(0.5 + d.y * d.y);
+        q.y = (float)d.y;
+    } else if constexpr (PK == PK_ERF) {
+        q.a1 = 0.f; q.p = 0.f;
+        q.y = (float)(0.5 * dx);
+    } else {
+        q.a1 = (float)(ampd * d.y * GEXS_INV_PI);
+        q.p = (float)(d.y * d.y);
+        q.y = (float)d.y;
+    }
+    q.pad = 0.f;
+    q.win = d.win; q.c1 = d.c1; q.c2 = d.c2; q.c3 = d.c3;
+}
+
+template <int PK>
+__device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const gexs_job& J)
+{
+    q.nu = d.nu; q.invw = d.invw; q.y = d.y;
+    q.amp = (PK == PK_ERF) ? d.S : dmul(d.S, d.invw);
+    q.win = d.win; q.c1 = d.c1; q.c2 = d.c2; q.c3 = d.c3;
+}
+
+/* ------------------------------------------------- per-warp line loops */
+template <int PK, int B>
+__device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nrec, int wb,
+                                          int lane, const float (&lk)[B], float (&part)[B],
+                                          int erf_form)
+{
+    const float wbf = (float)wb;
+    for (int i = 0; i < nrec; ++i) {
+        const RecF32& q = rec[i];
+        const int a = lo16(q.win), b = hi16(q.win);
+        if (b <= wb || a >= wb + 32 * B) continue;
+        const bool full = (a <= wb) && (b >= wb + 32 * B);
+        const float ncf = wbf - q.icf;
+        const int c1a = lo16(q.c1), c1b = hi16(q.c1);
+        if constexpr (PK == PK_VOIGT) {
+            const bool far = (c1a >= c1b) || (c1b <= wb) || (c1a >= wb + 32 * B);
+            if (full && far) {
+                /* every bin of the warp is in region I and in the window */
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    float x = fmaf(lk[k] + ncf, q.dx, q.mfcdx);
+                    float x2 = x * x;
+                    float num = x2 + q.p;
+                    float den = fmaf(x2, -2.f, num * num);
+                    part[k] = fmaf(num * rcp_approx(den), q.a1, part[k]);
+                }
+            } else {
+                const int c2 = q.c2, c3 = q.c3;
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = wb + lane + 32 * k;
+                    if (t < a || t >= b) continue;
+                    float x = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
+                    float v;
+                    if (t < c1a || t >= c1b) {
+                        float x2 = x * x;
+                        float num = x2 + q.p;
+                        float den = fmaf(x2, -2.f, num * num);
+                        v = num * rcp_approx(den) * q.a1;
+                    } else {
+                        int reg;
+                        if (t < lo16(c2) || t >= hi16(c2)) reg = 2;
+                        else reg = (t >= lo16(c3) && t < hi16(c3)) ? 3 : 4;
+                        v = q.amp * hum_by_region<float>(reg, x, q.y);
+                    }
+                    part[k] += v;
+                }
+            }
+        } else if constexpr (PK == PK_ERF) {
+            /* outside [c1a, c1b) every term is an exact zero */
+            if (c1a >= c1b || c1b <= wb || c1a >= wb + 32 * B) continue;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (t < a || t >= b || t < c1a || t >= c1b) continue;
+                float xd = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
+                part[k] = fmaf(q.amp, erf_bin_f32(xd - q.y, xd + q.y, erf_form), part[k]);
+            }
+        } else {
+            constexpr int NODES = (PK == PK_GH16) ? 16 : 32;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (!full && (t < a || t >= b)) continue;
+                float x = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
+                part[k] = fmaf(q.a1, gh_sum_f32<NODES>(x, q.p), part[k]);
+            }
+        }
+    }
+}
+
+template <int PK, int B>
+__device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nrec, int wb,
+                                          int lane, const double (&fbin)[B], double (&acc)[B],
+                                          const gexs_job& J)
+{
+    const double out_scale = J.out_scale;
+    for (int i = 0; i < nrec; ++i) {
+        const RecF64& q = rec[i];
+        const int a = lo16(q.win), b = hi16(q.win);
+        if (b <= wb || a >= wb + 32 * B) continue;
+        if constexpr (PK == PK_VOIGT) {
+            const int c1 = q.c1, c2 = q.c2, c3 = q.c3;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (t < a || t >= b) continue;
+                double x = dmul(fabs(dsub(fbin[k], q.nu)), q.invw);
+                int reg;
+                if (t < lo16(c1) || t >= hi16(c1)) reg = 1;
+                else if (t < lo16(c2) || t >= hi16(c2)) reg = 2;
+                else reg = (t >= lo16(c3) && t < hi16(c3)) ? 3 : 4;
+                double kv = hum_by_region<double>(reg, x, q.y);
+                acc[k] = dadd(acc[k], dmul(dmul(q.amp, kv), out_scale));
+            }
+        } else if constexpr (PK == PK_ERF) {
+            const int c1a = lo16(q.c1), c1b = hi16(q.c1);
+            if (c1a >= c1b || c1b <= wb || c1a >= wb + 32 * B) continue;
+            const int form = J.erf_form;
+            const double h = 0.5 * J.dnu;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (t < a || t >= b || t < c1a || t >= c1b) continue;
+                double dist = fabs(dsub(fbin[k], q.nu));
+                double xp = dmul(q.invw, dadd(dist, h));
+                double xm = dmul(q.invw, dsub(dist, h));
+                double de = erf_bin_f64(xm, xp, form);
+                acc[k] = dadd(acc[k], dmul(dmul(q.amp, de), out_scale));
+            }
+        } else {
+            constexpr int NODES = (PK == PK_GH16) ? 16 : 32;
+            const double y2 = dmul(q.y, q.y), yk = dmul(q.y, GEXS_INV_PI);
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (t < a || t >= b) continue;
+                double x = dmul(fabs(dsub(fbin[k], q.nu)), q.invw);
+                double kv = dmul(gh_sum_f64<NODES>(x, y2), yk);
+                acc[k] = dadd(acc[k], dmul(dmul(q.amp, kv), out_scale));
+            }
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- kernel */
+template <int PK, int PREC, int B, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+tile_kernel(const KArgs args)
+{
+    constexpr int NT = WARPS * 32;
+    constexpr int W = 32 * B * WARPS;
+    constexpr bool PRESS = (PK != PK_ERF);
+    typedef typename RecOf<PREC>::T Rec;
+
+    __shared__ double s_nu[2][NT];
+    __shared__ double s_el[2][NT];
+    __shared__ double s_ai[2][NT];
+    __shared__ double s_ga[2][PRESS ? NT : 1];
+    __shared__ double s_ne[2][PRESS ? NT : 1];
+    __shared__ int    s_gn[2][NT];
+    __shared__ Rec    s_rec[NT];
+    __shared__ int    s_item;
+    __shared__ long long s_lohi[2];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wb = warp * 32 * B;          /* warp's first bin (tile-relative) */
+    const double zthr = (PREC == GEXS_FP32) ? 10.5 : 27.5;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(args.counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= args.nitems) break;
+
+        /* job of this item: last prefix entry <= item */
+        int jl = 0, jh = args.njobs;
+        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= item) jl = m; else jh = m; }
+        const gexs_job* Jp = args.jobs + jl;
+        const gexs_job& J = *Jp;
+        Tile T;
+        T.J = Jp;
+        T.j0 = J.start_idx + (int64_t)(item - __ldg(args.prefix + jl)) * W;
+        T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
+        T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
+        T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
+
+        const int64_t nl = J.lines.count;
+        const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
+        if (warp == 0) {
+            int64_t v = warp_bound<false>(J.lines.nu, nl, T.f0 - J.cutoff - margin, lane);
+            if (lane == 0) s_lohi[0] = v;
+        } else if (warp == 1) {
+            int64_t v = warp_bound<true>(J.lines.nu, nl, T.fl + J.cutoff + margin, lane);
+            if (lane == 0) s_lohi[1] = v;
+        }
+        __syncthreads();
+        const int64_t lo = s_lohi[0];
+        const int64_t hi = max((int64_t)s_lohi[1], lo);
+        const int nst = (int)((hi - lo + NT - 1) / NT);
+
+        /* per-lane accumulators */
+        float  ks[B], kc[B], part[B], lk[B];
+        double acc[B], fbin[B];
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            ks[k] = kc[k] = part[k] = 0.f; acc[k] = 0.0;
+            lk[k] = (float)(lane + 32 * k);
+            fbin[k] = grid_f(J.nu_start, J.dnu, T.j0 + wb + lane + 32 * k);
+        }
+
+        auto issue = [&](int s) {
+            int64_t i = lo + (int64_t)s * NT + tid;
+            int buf = s & 1;
+            if (s < nst && i < hi) {
+                cp_async8(&s_nu[buf][tid], J.lines.nu + i);
+                cp_async8(&s_el[buf][tid], J.lines.elow + i);
+                cp_async8(&s_ai[buf][tid], J.lines.aif + i);
+                cp_async4(&s_gn[buf][tid], J.lines.gns + i);
+                if constexpr (PRESS) {
+                    cp_async8(&s_ga[buf][tid], J.lines.gamma + i);
+                    cp_async8(&s_ne[buf][tid], J.lines.n + i);
+                }
+            }
+            cp_async_commit();
+        };
+        issue(0);
+        issue(1);
+
+        for (int s = 0; s < nst; ++s) {
+            const int buf = s & 1;
+            cp_async_wait<1>();
+            __syncthreads();
+            const int nrec = (int)min((int64_t)NT, hi - lo - (int64_t)s * NT);
+            if (tid < nrec) {
+                RawLine L;
+                L.nu = s_nu[buf][tid]; L.elow = s_el[buf][tid]; L.aif = s_ai[buf][tid];
+                L.g = s_gn[buf][tid];
+                if constexpr (PRESS) { L.gam = s_ga[buf][tid]; L.nexp = s_ne[buf][tid]; }
+                else { L.gam = 0.0; L.nexp = 0.0; }
+                Derived<PK> d = derive_line<PK>(T, L, zthr);
+                Rec r;
+                make_rec<PK>(r, d, J);
+                s_rec[tid] = r;
+            }
+            __syncthreads();
+            issue(s + 2);
+
+            if constexpr (PREC == GEXS_FP32) {
+                lines_f32<PK, B>(s_rec, nrec, wb, lane, lk, part, J.erf_form);
+#pragma unroll
+                for (int k = 0; k < B; ++k) { kahan_add(ks[k], kc[k], part[k]); part[k] = 0.f; }
+            } else {
+                lines_f64<PK, B>(s_rec, nrec, wb, lane, fbin, acc, J);
+            }
+            __syncthreads();
+        }
+        cp_async_wait<0>();
+
+        /* ------------------------------------------------------- write out */
+        double* out = J.out;
+        const int acc_mode = J.accumulate;
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            const int t = wb + lane + 32 * k;
+            if (t < T.jn) {
+                double v = (PREC == GEXS_FP32) ? ((double)ks[k] - (double)kc[k]) : acc[k];
+                int64_t j = T.j0 + t;
+                out[j] = acc_mode ? out[j] + v : v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* ------------------------------------------------------ eval counting */
+__global__ void count_kernel(const gexs_job* __restrict__ jobs, unsigned long long* counts)
+{
+    const gexs_job& J = jobs[blockIdx.y];
+    unsigned long long local = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < J.lines.count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double nu = J.lines.nu[i];
+        if (nu == 0.0) nu = 1e-6;
+        int64_t s0 = J.start_idx, s1 = J.start_idx + J.n_points;
+        int64_t jl, jh;
+        if (J.window_rule == GEXS_WINDOW_ROUNDED) {
+            double ib = round(ddiv(dsub(dsub(nu, J.cutoff), J.nu_start), J.dnu));
+            double ie = round(ddiv(dsub(dadd(nu, J.cutoff), J.nu_start), J.dnu));
+            ib = fmax(ib, (double)s0); ie = fmin(ie, (double)s1);
+            jl = (int64_t)ib; jh = (int64_t)ie; if (jh < jl) jh = jl;
+        } else {
+            auto in = [&](int64_t j) { return fabs(dsub(grid_f(J.nu_start, J.dnu, j), nu)) <= J.cutoff; };
+            double c = ddiv(dsub(nu, J.nu_start), J.dnu), w = ddiv(J.cutoff, J.dnu);
+            double le = floor(c - w) - 2.0, he = ceil(c + w) + 2.0;
+            jl = (int64_t)fmax((double)s0, fmin(le, (double)s1));
+            jh = (int64_t)fmax((double)s0, fmin(he, (double)s1));
+            int guard = 0;
+            while (jl > s0 && in(jl - 1) && guard++ < 64) --jl;
+            while (jl < jh && !in(jl) && guard++ < 128) ++jl;
+            while (jh < s1 && in(jh) && guard++ < 192) ++jh;
+            while (jh > jl && !in(jh - 1) && guard++ < 256) --jh;
+        }
+        local += (unsigned long long)(jh - jl);
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(counts + blockIdx.y, local);
+}
+
+/* ------------------------------------------------ partition function Q(T) */
+__global__ void partition_partial(const double* __restrict__ e, const int32_t* __restrict__ g,
+                                  int64_t n, const double* __restrict__ betas, double* partial)
+{
+    /* block (x = chunk, y = temperature); fixed-order tree reduction */
+    __shared__ double red[256];
+    const double beta = betas[blockIdx.y];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        s += (double)g[i] * exp(-beta * e[i]);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
+__global__ void partition_final(const double* partial, int nchunk, int nt, double* q)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    double s = 0.0;
+    for (int c = 0; c < nchunk; ++c) s += partial[t * nchunk + c];
+    q[t] = s;
+}
+
+/* ------------------------------------------------------------ dispatch */
+template <int PK, int PREC, int B, int WARPS>
+static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st)
+{
+    auto kern = tile_kernel<PK, PREC, B, WARPS>;
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, WARPS * 32, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) occ = 1;
+    int per = ctas_per_sm > 0 ? min(ctas_per_sm, occ) : occ;
+    int grid = min(a.nitems, per * nsm);
+    if (grid < 1) grid = 1;
+    kern<<<grid, WARPS * 32, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int PK, int PREC>
+static cudaError_t launch_cfg(const KArgs& a, const gexs_launch_cfg& c, int nsm, cudaStream_t st)
+{
+    if (c.warps == 8) {
+        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 8>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 8>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 8>(a, c.ctas_per_sm, nsm, st);
+    } else if (c.warps == 4) {
+        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 4>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 4>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 4>(a, c.ctas_per_sm, nsm, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+int profile_class(const gexs_job& j)
+{
+    if (j.profile == GEXS_VOIGT) return PK_VOIGT;
+    if (j.profile == GEXS_DOPPLER || j.profile == GEXS_GAUSSIAN) return PK_ERF;
+    if (j.profile == GEXS_VOIGT_QUAD) return j.quad_nodes == 16 ? PK_GH16 : PK_GH32;
+    return -1;
+}
+
+cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
+                         int njobs, int nitems, int* d_counter, int* d_err,
+                         const gexs_launch_cfg& cfg, int nsm, cudaStream_t st)
+{
+    KArgs a;
+    a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
+    a.counter = d_counter; a.err = d_err;
+    if (prec == GEXS_FP32) {
+        switch (pk) {
+        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP32>(a, cfg, nsm, st);
+        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP32>(a, cfg, nsm, st);
+        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP32>(a, cfg, nsm, st);
+        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP32>(a, cfg, nsm, st);
+        }
+    } else {
+        switch (pk) {
+        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP64>(a, cfg, nsm, st);
+        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP64>(a, cfg, nsm, st);
+        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP64>(a, cfg, nsm, st);
+        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP64>(a, cfg, nsm, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+int tile_bins(const gexs_launch_cfg& c) { return 32 * c.bins_per_lane * c.warps; }
+
+cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,
+                         int nsm, cudaStream_t st)
+{
+    dim3 grid(nsm * 4, njobs);
+    count_kernel<<<grid, 256, 0, st>>>(d_jobs, d_counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,
+                             const double* d_betas, int nt, double* d_partial, int nchunk,
+                             double* d_q, cudaStream_t st)
+{
+    dim3 grid(nchunk, nt);
+    partition_partial<<<grid, 256, 0, st>>>(d_e, d_g, n, d_betas, d_partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    partition_final<<<(nt + 127) / 128, 128, 0, st>>>(d_partial, nchunk, nt, d_q);
+    return cudaGetLastError();
+}
+
+}  // namespace gexs

@@ -1,0 +1,253 @@
+"""Python view of the engine's C ABI (device memory via torch tensors).
+
+The product path is the C ABI in libgexs_b200.so; this module only packs
+descriptors and keeps the tensors they point at alive.
+"""
+import ctypes as C
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check, lib
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+class LineList:
+    """Device-resident line list (structure of arrays, sorted by nu)."""
+
+    def __init__(self, nu, elow, aif, gns, gamma=None, n=None, device="cuda"):
+        import torch
+        def to(a, dt):
+            if a is None:
+                return None
+            return torch.as_tensor(a, dtype=dt).to(device).contiguous()
+        self.nu = to(nu, torch.float64)
+        self.elow = to(elow, torch.float64)
+        self.aif = to(aif, torch.float64)
+        self.gns = to(gns, torch.int32)
+        self.gamma = to(gamma, torch.float64)
+        self.n = to(n, torch.float64)
+        self.count = int(self.nu.shape[0])
+
+    @classmethod
+    def from_dict(cls, d, device="cuda"):
+        return cls(d["nu"], d["elow"], d["aif"], d["gns"], d.get("gamma"), d.get("n"), device)
+
+    def c_lines(self):
+        return capi.GexsLines(_ptr(self.nu), _ptr(self.elow), _ptr(self.aif), _ptr(self.gns),
+                              _ptr(self.gamma), _ptr(self.n), self.count)
+
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in
+                   (self.nu, self.elow, self.aif, self.gns, self.gamma, self.n) if t is not None)
+
+
+def job_init(convention, profile, temperature, pressure, partition, mass, nu_start, dnu,
+             grid_points, ref_temp=296.0, ref_press=1.0, half_width=0.0, cutoff=-1.0):
+    """gexs_job_init: physics constants of a convention (no pointers set)."""
+    j = capi.GexsJob()
+    check(lib().gexs_job_init(C.byref(j), convention, profile, temperature, pressure, partition,
+                              mass, ref_temp, ref_press, half_width, cutoff, nu_start, dnu,
+                              int(grid_points)), "gexs_job_init")
+    return j
+
+
+class Job:
+    """One cross-section job: a GexsJob plus the tensors it references."""
+
+    def __init__(self, lines, out, *, convention, profile, temperature, pressure, partition,
+                 mass, nu_start, dnu, grid_points, precision=capi.FP32, ref_temp=296.0,
+                 ref_press=1.0, half_width=0.0, cutoff=-1.0, start_idx=0, n_points=None,
+                 accumulate=0, quad_nodes=16, window_rule=None, erf_form=None):
+        self.c = job_init(convention, profile, temperature, pressure, partition, mass,
+                          nu_start, dnu, grid_points, ref_temp, ref_press, half_width, cutoff)
+        self.lines = lines
+        self.out = out
+        self.c.lines = lines.c_lines()
+        self.c.out = out.data_ptr()
+        self.c.precision = precision
+        self.c.start_idx = start_idx
+        self.c.n_points = grid_points - start_idx if n_points is None else n_points
+        self.c.accumulate = accumulate
+        self.c.quad_nodes = quad_nodes
+        if window_rule is not None:
+            self.c.window_rule = window_rule
+        if erf_form is not None:
+            self.c.erf_form = erf_form
+
+    def host_copy(self, host_lines):
+        """The same job pointing at host numpy arrays (for the oracle)."""
+        j = capi.GexsJob.from_buffer_copy(self.c)
+        hl = host_lines
+        def p(a):
+            return None if a is None else a.ctypes.data_as(C.c_void_p)
+        j.lines = capi.GexsLines(p(hl["nu"]), p(hl["elow"]), p(hl["aif"]), p(hl["gns"]),
+                                 p(hl.get("gamma")), p(hl.get("n")), len(hl["nu"]))
+        j.out = None
+        return j
+
+
+def _job_array(jobs):
+    arr = (capi.GexsJob * len(jobs))()
+    for i, j in enumerate(jobs):
+        arr[i] = j.c if isinstance(j, Job) else j
+    return arr
+
+
+def _cfg(cfg):
+    if cfg is None:
+        return None
+    if isinstance(cfg, capi.GexsLaunchCfg):
+        return C.byref(cfg)
+    b, w, c = cfg
+    return C.byref(capi.GexsLaunchCfg(b, w, c, 0))
+
+
+class Batch:
+    def __init__(self, ctx, jobs, cfg=None):
+        self._jobs = list(jobs)
+        self.h = C.c_void_p()
+        arr = _job_array(self._jobs)
+        check(lib().gexs_batch_create(ctx.h, arr, len(arr), _cfg(cfg), C.byref(self.h)),
+              "gexs_batch_create")
+
+    def launch(self, stream=None):
+        check(lib().gexs_batch_launch(self.h, _stream_handle(stream)), "gexs_batch_launch")
+
+    def capture(self, stream):
+        check(lib().gexs_batch_capture(self.h, _stream_handle(stream)), "gexs_batch_capture")
+
+    def replay(self, stream=None):
+        check(lib().gexs_batch_replay(self.h, _stream_handle(stream)), "gexs_batch_replay")
+
+    def close(self):
+        if self.h:
+            lib().gexs_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    def __init__(self, device=0):
+        self.h = C.c_void_p()
+        check(lib().gexs_ctx_create(device, C.byref(self.h)), "gexs_ctx_create")
+
+    def close(self):
+        if self.h:
+            lib().gexs_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, jobs, cfg=None, stream=None):
+        arr = _job_array(jobs)
+        check(lib().gexs_run(self.h, arr, len(arr), _cfg(cfg), _stream_handle(stream)), "gexs_run")
+
+    def check(self, stream=None):
+        check(lib().gexs_ctx_check(self.h, _stream_handle(stream)), "gexs_ctx_check")
+
+    def count_evals(self, jobs):
+        arr = _job_array(jobs)
+        out = (C.c_int64 * len(arr))()
+        check(lib().gexs_count_evals(self.h, arr, len(arr), out), "gexs_count_evals")
+        return [int(v) for v in out]
+
+    def batch(self, jobs, cfg=None):
+        return Batch(self, jobs, cfg)
+
+    def autotune(self, jobs):
+        arr = _job_array(jobs)
+        best = capi.GexsLaunchCfg()
+        ms = C.c_float()
+        check(lib().gexs_autotune(self.h, arr, len(arr), C.byref(best), C.byref(ms)),
+              "gexs_autotune")
+        return (best.bins_per_lane, best.warps, best.ctas_per_sm), float(ms.value)
+
+    def partition(self, energy, g, temps):
+        temps = np.ascontiguousarray(temps, dtype=np.float64)
+        q = np.zeros_like(temps)
+        check(lib().gexs_partition(self.h, _ptr(energy), _ptr(g), int(energy.shape[0]),
+                                   temps.ctypes.data_as(C.POINTER(C.c_double)), len(temps),
+                                   q.ctypes.data_as(C.POINTER(C.c_double))), "gexs_partition")
+        return q
+
+
+class Manager:
+    """The drop-in BaseManager (B200Manager) through its flat C wrappers;
+    host numpy arrays in and out, exactly as BaseProfile passes them."""
+
+    def __init__(self, profile, device=0, convention=capi.CONV_REF_GPU, precision=capi.FP64,
+                 memory_bytes=0):
+        self.h = C.c_void_p()
+        check(lib().gexs_manager_create(profile, device, convention, precision, memory_bytes,
+                                        C.byref(self.h)), "gexs_manager_create")
+
+    def close(self):
+        if self.h:
+            lib().gexs_manager_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _p(a):
+        return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+    def initialize_vectors(self, npoints, num_cs):
+        check(lib().gexs_manager_initialize_vectors(self.h, npoints, num_cs), "InitializeVectors")
+
+    def initialize_constants(self, half_width, temperature, partition, dfreq, meanmass,
+                             pressure=10.0, ref_temp=296.0, ref_press=1.0):
+        check(lib().gexs_manager_initialize_constants(self.h, half_width, temperature, partition,
+                                                      dfreq, meanmass, pressure, ref_temp,
+                                                      ref_press), "InitializeConstants")
+
+    def transfer_freq(self, freq, intens):
+        check(lib().gexs_manager_transfer_freq(self.h, self._p(freq), self._p(intens), len(freq)),
+              "TransferFreq")
+
+    def transfer_vectors(self, energies, nu, aif, gns, gamma=None, n=None):
+        check(lib().gexs_manager_transfer_vectors(self.h, len(nu), self._p(energies), self._p(nu),
+                                                  self._p(aif), self._p(gns), self._p(gamma),
+                                                  self._p(n)), "TransferVectors")
+
+    def execute(self, n, n_ener, start_idx, temperature, pressure, partition):
+        check(lib().gexs_manager_execute(self.h, n, n_ener, start_idx, temperature, pressure,
+                                         partition), "ExecuteCrossSection")
+
+    def transfer_results(self, freq, intens, i):
+        check(lib().gexs_manager_transfer_results(self.h, self._p(freq), self._p(intens),
+                                                  len(intens), i), "TransferResults")
+
+    def ntrans(self):
+        v = C.c_size_t()
+        check(lib().gexs_manager_ntrans(self.h, C.byref(v)), "GetNtrans")
+        return int(v.value)
+
+    def ready(self):
+        v = C.c_int()
+        check(lib().gexs_manager_ready(self.h, C.byref(v)), "ReadyForWork")
+        return bool(v.value)

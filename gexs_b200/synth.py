@@ -1,0 +1,122 @@
+"""Seeded synthetic ExoMol-style line lists (the workloads have no public
+dataset; these stand in with the stated shapes and distributions).
+
+States: E ~ Exponential(mean 4000 cm^-1) clipped to [0, 30000], J uniform
+integer in [0, j_max], g = 2J + 1.  Transitions: the lower state is uniform
+over states; the upper state is uniform over states with
+E_u in [E_l + nu_min, E_l + nu_max] (lower states with no such upper state
+are redrawn); nu0 = E_u - E_l; Einstein A log-uniform in [1e-6, 1e2] s^-1;
+g_ns of the line = g of the upper state (Readers/Exomol/
+ExomolStateReader.cpp:158-162 takes energy of the lower state and g of the
+upper).  Broadening: gamma_ref ~ U(0.03, 0.1) cm^-1/atm, n ~ U(0.4, 0.8).
+Lines are returned sorted by nu0.
+
+numpy (PCG64) is used for CPU-sized lists; the torch variant generates the
+same distributions on the GPU for 1e8-line lists (different random stream).
+"""
+import numpy as np
+
+
+class States:
+    def __init__(self, energy, g, j):
+        self.energy = energy
+        self.g = g
+        self.j = j
+
+
+def make_states(n, j_max, seed, mean_e=4000.0, e_max=30000.0):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    e = np.clip(rng.exponential(mean_e, n), 0.0, e_max)
+    j = rng.integers(0, j_max + 1, n).astype(np.int32)
+    return States(e.astype(np.float64), (2 * j + 1).astype(np.int32), j)
+
+
+def _pick_upper(rng, es, lower_e, nu_min, nu_max):
+    lo = np.searchsorted(es, lower_e + nu_min, side="left")
+    hi = np.searchsorted(es, lower_e + nu_max, side="right")
+    ok = hi > lo
+    u = rng.random(lower_e.shape[0])
+    up = lo + np.floor(u * np.maximum(hi - lo, 1)).astype(np.int64)
+    up = np.minimum(up, len(es) - 1)
+    return up, ok
+
+
+def make_lines(states, ntrans, nu_min, nu_max, seed, broadening_seed=None):
+    """Return dict of numpy arrays nu, elow, aif, gns (+ gamma, n when
+    broadening_seed is given), sorted by nu."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    order = np.argsort(states.energy, kind="stable")
+    es = states.energy[order]
+    gs = states.g[order]
+    n = len(es)
+    low = rng.integers(0, n, ntrans)
+    up, ok = _pick_upper(rng, es, es[low], nu_min, nu_max)
+    for _ in range(64):
+        bad = np.nonzero(~ok)[0]
+        if bad.size == 0:
+            break
+        low[bad] = rng.integers(0, n, bad.size)
+        u2, ok2 = _pick_upper(rng, es, es[low[bad]], nu_min, nu_max)
+        up[bad] = u2
+        ok[bad] = ok2
+    keep = ok
+    low, up = low[keep], up[keep]
+    nu = es[up] - es[low]
+    aif = 10.0 ** rng.uniform(-6.0, 2.0, nu.shape[0])
+    srt = np.argsort(nu, kind="stable")
+    out = {
+        "nu": np.ascontiguousarray(nu[srt], dtype=np.float64),
+        "elow": np.ascontiguousarray(es[low][srt], dtype=np.float64),
+        "aif": np.ascontiguousarray(aif[srt], dtype=np.float64),
+        "gns": np.ascontiguousarray(gs[up][srt], dtype=np.int32),
+    }
+    if broadening_seed is not None:
+        r2 = np.random.Generator(np.random.PCG64(broadening_seed))
+        out["gamma"] = r2.uniform(0.03, 0.1, nu.shape[0]).astype(np.float64)
+        out["n"] = r2.uniform(0.4, 0.8, nu.shape[0]).astype(np.float64)
+    return out
+
+
+def make_lines_torch(states, ntrans, nu_min, nu_max, seed, broadening_seed=None,
+                     device="cuda"):
+    """Same distributions generated with torch on `device` (for 1e8+ lines).
+    Returns dict of torch tensors sorted by nu."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    order = np.argsort(states.energy, kind="stable")
+    es = torch.as_tensor(states.energy[order], device=device)
+    gs = torch.as_tensor(states.g[order], device=device)
+    n = es.shape[0]
+    low = torch.randint(0, n, (ntrans,), generator=gen, device=device)
+    el = es[low]
+    lo = torch.searchsorted(es, el + nu_min, side="left")
+    hi = torch.searchsorted(es, el + nu_max, side="right")
+    ok = hi > lo
+    for _ in range(64):
+        bad = torch.nonzero(~ok).flatten()
+        if bad.numel() == 0:
+            break
+        low[bad] = torch.randint(0, n, (bad.numel(),), generator=gen, device=device)
+        el[bad] = es[low[bad]]
+        lo[bad] = torch.searchsorted(es, el[bad] + nu_min, side="left")
+        hi[bad] = torch.searchsorted(es, el[bad] + nu_max, side="right")
+        ok[bad] = hi[bad] > lo[bad]
+    u = torch.rand(ntrans, generator=gen, device=device, dtype=torch.float64)
+    up = lo + torch.floor(u * (hi - lo).clamp(min=1).double()).long()
+    up = up.clamp(max=n - 1)
+    keep = torch.nonzero(ok).flatten()
+    low, up = low[keep], up[keep]
+    nu = es[up] - es[low]
+    aif = torch.pow(10.0, torch.empty(nu.shape[0], device=device, dtype=torch.float64)
+                    .uniform_(-6.0, 2.0, generator=gen))
+    nu_sorted, srt = torch.sort(nu, stable=True)
+    out = {"nu": nu_sorted.contiguous(), "elow": es[low][srt].contiguous(),
+           "aif": aif[srt].contiguous(), "gns": gs[up][srt].to(torch.int32).contiguous()}
+    if broadening_seed is not None:
+        g2 = torch.Generator(device=device)
+        g2.manual_seed(int(broadening_seed))
+        m = nu.shape[0]
+        out["gamma"] = torch.empty(m, device=device, dtype=torch.float64).uniform_(0.03, 0.1, generator=g2)
+        out["n"] = torch.empty(m, device=device, dtype=torch.float64).uniform_(0.4, 0.8, generator=g2)
+    return out

@@ -1,0 +1,243 @@
+/*
+ * gexs_b200.h — C ABI of the B200 (sm_100a) cross-section engine.
+ *
+ * The engine computes molecular absorption cross-sections: for every line
+ * (transition) it derives the intensity S(T) and a line width, then sums a
+ * Doppler, Gaussian, Voigt (Humlicek W4) or Voigt-Quad (Gauss-Hermite)
+ * profile onto a uniform wavenumber grid.  It is the compute path that the
+ * reference GEXS reaches through its manager plug-in interface
+ * (Managers/BaseManager.h:6-38): BaseProfile::PerformCrossSection
+ * (Profiles/BaseProfile.cpp:100-116) hands a chunk of lines to
+ * BaseManager::TransferVectors and then calls
+ * BaseManager::ExecuteCrossSection once per (T, P) pair.
+ *
+ * Every function returns an int status: GEXS_OK (0) or a negative GEXS_ERR_*
+ * code; gexs_last_error() gives a message for the calling thread.  No
+ * function prints or exits (the reference prints and calls exit(-1),
+ * compute/CUDA/cuda_utils.cu:8-17).  Pointers named d_* / fields documented
+ * as device pointers refer to CUDA device memory of the context's device;
+ * h_* are host pointers.  `stream` is a cudaStream_t passed as void*
+ * (NULL = the legacy default stream).
+ */
+#ifndef GEXS_B200_H
+#define GEXS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define GEXS_OK              0
+#define GEXS_ERR_INVALID    -1  /* bad argument or unsupported combination    */
+#define GEXS_ERR_OOM        -2  /* device or host allocation failed           */
+#define GEXS_ERR_CUDA       -3  /* a CUDA runtime call failed                 */
+#define GEXS_ERR_TIMEOUT    -4  /* a bounded wait ran out                     */
+#define GEXS_ERR_NOT_READY  -5  /* asynchronous result not available yet      */
+#define GEXS_ERR_ADMISSION  -6  /* request exceeds the memory budget          */
+#define GEXS_ERR_SHUTDOWN   -7  /* object is shutting down                    */
+#define GEXS_ERR_KERNEL     -8  /* a kernel reported an internal error flag   */
+
+/* --------------------------------------------------------------- profiles
+ * Values of GAUSSIAN, DOPPLER, VOIGT and VOIGT_QUAD equal the reference's
+ * ProfileType enum (common/Input.h:10-17) so a ProfileType converts 1:1. */
+#define GEXS_GAUSSIAN    0  /* fixed half-width Gaussian, bin-averaged        */
+#define GEXS_DOPPLER     1  /* thermal Gaussian, bin-averaged                 */
+#define GEXS_VOIGT       2  /* Humlicek W4 Faddeeva real part                 */
+#define GEXS_VOIGT_QUAD  4  /* Gauss-Hermite quadrature Voigt (16/32 nodes)   */
+
+/* precision of the profile arithmetic */
+#define GEXS_FP64  0  /* plain FP64 throughout                                 */
+#define GEXS_FP32  1  /* FP64 line centres/S(T)/Q(T); FP32 profile; Kahan bins */
+
+/* which grid bins a line reaches */
+#define GEXS_WINDOW_INCLUSIVE 0 /* bins j with |f_j - nu0| <= cutoff (FP64)    */
+#define GEXS_WINDOW_ROUNDED   1 /* [round((nu0-cut-f_0)/dnu), round((nu0+cut-f_0)/dnu))
+                                   as Managers/CPU/OpenMPManager.cpp:399-400    */
+
+/* form of the bin-averaged erf difference (Doppler, Gaussian) */
+#define GEXS_ERF_STABLE   0 /* erfc(xm)-erfc(xp) when xm>=0: no cancellation  */
+#define GEXS_ERF_LITERAL  1 /* erf(xp)-erf(xm) exactly as the reference       */
+
+/* conventions reproduced by gexs_job_init (see that function) */
+#define GEXS_CONV_PHYSICAL 0
+#define GEXS_CONV_REF_CPU  1
+#define GEXS_CONV_REF_GPU  2
+
+/* ------------------------------------------------------------- line lists
+ * Structure-of-arrays, exactly the arrays BaseManager::TransferVectors
+ * receives (Managers/BaseManager.h:26).  Lines must be sorted by nu
+ * ascending (BaseProfile.cpp:152-155 relies on the same order).  gamma and
+ * n may be NULL for profiles that do not use pressure broadening. */
+typedef struct gexs_lines {
+    const double*  nu;     /* line centre nu0 [cm^-1]                      */
+    const double*  elow;   /* lower-state energy [cm^-1]                   */
+    const double*  aif;    /* Einstein A coefficient [s^-1]                */
+    const int32_t* gns;    /* upper-state degeneracy                       */
+    const double*  gamma;  /* Lorentz half-width at T_ref, 1 atm [cm^-1]   */
+    const double*  n;      /* temperature exponent of gamma                */
+    int64_t        count;
+} gexs_lines;
+
+/* ------------------------------------------------------------------ jobs
+ * One cross-section: one line list, one (T, P), one grid.  Bins
+ * [start_idx, start_idx + n_points) of the grid f_j = nu_start + j*dnu
+ * (j in [0, grid_points), evaluated without fused multiply-add, like
+ * BaseProfile.cpp:17-21) are written to out[j].
+ *
+ * Per line (nu0 == 0 is replaced by 1e-6, OpenMPManager.cpp:392):
+ *   S      = ((((s_scale*A)*g)*s_scale2)*exp(-beta*E)) * (1-exp(-beta*nu0))
+ *            / ((nu0*nu0)*partition)
+ *   invw   = 1/(nu0*dop_coef)           (Doppler, Voigt, Voigt-Quad)
+ *          = inv_width                  (Gaussian)
+ *   gammaL = (gamma * t_ratio^n) * gamma_scale
+ *   y      = gammaL * invw
+ *   Voigt:      term_j = ((S*K(x_j,y))*invw)*out_scale, x_j = |f_j-nu0|*invw
+ *   Voigt-Quad: same with K = Gauss-Hermite K_N
+ *   Doppler, Gaussian: term_j = (S*(erf(xp)-erf(xm)))*out_scale,
+ *               xp = invw*(|f_j-nu0|+dnu/2), xm = invw*(|f_j-nu0|-dnu/2)
+ *   out[j] = (accumulate ? out[j] : 0) + sum over lines in nu order of term_j
+ */
+typedef struct gexs_job {
+    gexs_lines lines;        /* device pointers                                   */
+    double*    out;          /* device, grid_points doubles                        */
+    double     nu_start;     /* f_0 [cm^-1]                                        */
+    double     dnu;          /* grid spacing [cm^-1]                               */
+    int64_t    grid_points;
+    int64_t    start_idx;
+    int64_t    n_points;
+    int32_t    profile;      /* GEXS_GAUSSIAN / DOPPLER / VOIGT / VOIGT_QUAD       */
+    int32_t    precision;    /* GEXS_FP64 / GEXS_FP32                              */
+    int32_t    window_rule;  /* GEXS_WINDOW_*                                      */
+    int32_t    accumulate;   /* 0 overwrite, 1 add into out                        */
+    int32_t    quad_nodes;   /* 16 or 32 (GEXS_VOIGT_QUAD)                         */
+    int32_t    erf_form;     /* GEXS_ERF_*                                         */
+    double     cutoff;       /* window half-width [cm^-1]                          */
+    double     partition;    /* Q(T)                                               */
+    double     beta;         /* h c / (k T) [cm]                                   */
+    double     s_scale;      /* first intensity prefactor                          */
+    double     s_scale2;     /* second intensity prefactor                         */
+    double     dop_coef;     /* Doppler width per cm^-1 of nu0                     */
+    double     inv_width;    /* Gaussian 1/width                                   */
+    double     t_ratio;      /* T_ref / T                                          */
+    double     gamma_scale;  /* pressure factor of gammaL                          */
+    double     out_scale;    /* final multiplier of each term                      */
+} gexs_job;
+
+/* Fill a job's physics constants for one of three conventions.  Grid,
+ * lines, out, precision and accumulate are left for the caller.
+ *  GEXS_CONV_PHYSICAL: 1/e Doppler half-width alpha = nu0/c*sqrt(2kT N_A/m),
+ *     gammaL = gamma*(T_ref/T)^n*(P[bar]/1.01325), inclusive window at
+ *     `cutoff`, Voigt out_scale = 1/sqrt(pi), Doppler/Gaussian 0.5/dnu.
+ *  GEXS_CONV_REF_CPU: Managers/CPU/OpenMPManager.cpp:280-323 (Doppler) and
+ *     :376-426 (Voigt): HWHM Doppler scaling, no pressure factor, cutoff
+ *     min(25P,100) (Doppler 100, common/defines.h:16), rounded window,
+ *     1/sqrt(pi) folded into S, literal erf difference, no 0.5/dnu.
+ *  GEXS_CONV_REF_GPU: compute/CUDA/cross_kernal_v2.cu:111-146,330-457 with
+ *     constants of Managers/Accel/GPU/GPUManager.cpp:29-49.
+ * cutoff < 0 selects the convention's default cutoff.  half_width is the
+ * Gaussian HWHM (GEXS_GAUSSIAN only). */
+int gexs_job_init(gexs_job* job, int convention, int profile,
+                  double temperature, double pressure, double partition,
+                  double mean_mass, double ref_temp, double ref_press,
+                  double half_width, double cutoff,
+                  double nu_start, double dnu, int64_t grid_points);
+
+/* --------------------------------------------------------------- context */
+typedef struct gexs_ctx gexs_ctx;
+
+typedef struct gexs_launch_cfg {
+    int32_t bins_per_lane;   /* 2, 4 or 8                       */
+    int32_t warps;           /* 4 or 8 (tile = 32*bins*warps)   */
+    int32_t ctas_per_sm;     /* resident CTAs per SM (>=1)      */
+    int32_t reserved;
+} gexs_launch_cfg;
+
+int         gexs_ctx_create(int device, gexs_ctx** out);
+int         gexs_ctx_destroy(gexs_ctx* ctx);
+const char* gexs_status_string(int status);
+const char* gexs_last_error(void);
+int         gexs_version(void);
+
+/* Run njobs jobs (host array of descriptors holding device pointers) on
+ * `stream`: one persistent launch over every (job, tile) work item.
+ * cfg NULL = the context's tuned default for the jobs' profile/precision.
+ * Asynchronous; kernel error flags are checked by gexs_ctx_check. */
+int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+             const gexs_launch_cfg* cfg, void* stream);
+
+/* Synchronise `stream` and read the context's kernel error flag. */
+int gexs_ctx_check(gexs_ctx* ctx, void* stream);
+
+/* Exact number of (line, bin) profile evaluations of each job (the window
+ * rule applied to every line): counts[i] for jobs[i]. Synchronous. */
+int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+                     int64_t* h_counts);
+
+/* ------------------------------------------------------ batched launches
+ * A batch owns its device job table and work-item table; launching it is
+ * one memset of the work counter plus one persistent kernel, which can be
+ * captured once into a CUDA graph and replayed. */
+typedef struct gexs_batch gexs_batch;
+
+int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+                      const gexs_launch_cfg* cfg, gexs_batch** out);
+int gexs_batch_launch(gexs_batch* b, void* stream);
+int gexs_batch_capture(gexs_batch* b, void* stream);  /* build the graph   */
+int gexs_batch_replay(gexs_batch* b, void* stream);   /* launch the graph  */
+int gexs_batch_destroy(gexs_batch* b);
+
+/* Pick bins_per_lane / warps / ctas_per_sm for these jobs by timing each
+ * candidate (CUDA events) on the jobs themselves.  Writes the winner to
+ * *best and records it as the context default for the jobs' profile and
+ * precision; h_ms (may be NULL) gets the winner's time. */
+int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+                  gexs_launch_cfg* best, float* h_ms);
+
+/* ------------------------------------------------------ partition function
+ * Q(T) = sum_s g_s exp(-c2 E_s / T) in FP64 for nt temperatures
+ * (Readers/Exomol/exomol_functions.cpp:50-73), states resident on device. */
+int gexs_partition(gexs_ctx* ctx, const double* d_energy, const int32_t* d_g,
+                   int64_t nstates, const double* h_temps, int nt,
+                   double* h_q);
+
+/* ------------------------------------------------------------ manager ABI
+ * Flat C view of the drop-in manager (B200Manager, a BaseManager subclass):
+ * one function per BaseManager virtual (Managers/BaseManager.h:22-35) so an
+ * FFI caller can drive it exactly as BaseProfile drives a manager. */
+typedef struct gexs_manager gexs_manager;
+
+int gexs_manager_create(int profile, int device, int convention,
+                        int precision, size_t memory_bytes,
+                        gexs_manager** out);
+int gexs_manager_destroy(gexs_manager* m);
+/* BaseManager::InitializeVectors(int Npoints, int num_cs) */
+int gexs_manager_initialize_vectors(gexs_manager* m, int npoints, int num_cs);
+/* BaseManager::InitializeConstants(...) */
+int gexs_manager_initialize_constants(gexs_manager* m, double half_width,
+        double temperature, double partition, double dfreq, double meanmass,
+        double pressure, double ref_temp, double ref_press);
+/* BaseManager::TransferFreq(double* h_freq, double* h_intens, int N) */
+int gexs_manager_transfer_freq(gexs_manager* m, const double* h_freq,
+                               const double* h_intens, int n);
+/* BaseManager::TransferVectors(...) */
+int gexs_manager_transfer_vectors(gexs_manager* m, size_t nener,
+        const double* h_energies, const double* h_nu, const double* h_aif,
+        const int* h_gns, const double* h_gamma, const double* h_n);
+/* BaseManager::ExecuteCrossSection(N, N_ener, start_idx, T, P, Q) */
+int gexs_manager_execute(gexs_manager* m, int n, int n_ener, int start_idx,
+                         double temperature, double pressure,
+                         double partition);
+/* BaseManager::TransferResults(h_freq, h_intens, N, I) */
+int gexs_manager_transfer_results(gexs_manager* m, double* h_freq,
+                                  double* h_intens, int n, int i);
+/* BaseManager::GetNtrans() and ReadyForWork() */
+int gexs_manager_ntrans(gexs_manager* m, size_t* out);
+int gexs_manager_ready(gexs_manager* m, int* ready);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEXS_B200_H */
