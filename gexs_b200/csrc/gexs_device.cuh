@@ -181,6 +181,21 @@ __device__ __forceinline__ float gh_sum_f32(float x, float y2)
     return acc;
 }
 
+/* same sum as 1/A + 1/B per pair: no A*B product, safe for |x| > 1e9 */
+template <int NODES>
+__device__ __forceinline__ float gh_sum_f32_wide(float x, float y2)
+{
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < GH<NODES>::NP; ++k) {
+        float t = (float)gh_t<NODES>(k), w = (float)gh_w<NODES>(k);
+        float d1 = x - t, d2 = x + t;
+        float A = fmaf(d1, d1, y2), B = fmaf(d2, d2, y2);
+        acc = fmaf(w, 1.f / A + 1.f / B, acc);
+    }
+    return acc;
+}
+
 template <int NODES>
 __device__ __forceinline__ double gh_sum_f64(double x, double y2)
 {

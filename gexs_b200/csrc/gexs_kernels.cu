@@ -38,7 +38,8 @@ struct RecF32 {            /* 48 bytes */
     float p;               /* Voigt: 0.5 + y^2 ; GH: y^2                     */
     float y;               /* Voigt/GH: y ; Doppler: half bin in x units     */
     float amp;             /* Voigt/GH: S*invw*out_scale ; Doppler: S*out    */
-    float pad;
+    int   wide;            /* 1: |x| may exceed 1e8 in this tile; use the
+                              overflow-free forms                            */
     int   win;             /* a | b << 16 : bins [a, b) of the tile          */
     int   c1;              /* Voigt: bins not in region I ; Doppler: bins
                               whose xm <= zero threshold                     */
@@ -258,7 +259,8 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
 
 /* --------------------------------------------------------- record builders */
 template <int PK>
-__device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const gexs_job& J)
+__device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const gexs_job& J,
+                                         const Tile& T)
 {
     double ic = floor(d.tc);
     ic = fmin(fmax(ic, -8388608.0), 8388607.0);
@@ -281,12 +283,17 @@ __device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const 
         q.p = (float)(d.y * d.y);
         q.y = (float)d.y;
     }
-    q.pad = 0.f;
+    {
+        /* largest |x| the line reaches in this tile */
+        double dfar = fmax(fabs(d.nu - T.f0), fabs(d.nu - T.fl));
+        q.wide = (dfar * d.invw > 1e8) ? 1 : 0;
+    }
     q.win = d.win; q.c1 = d.c1; q.c2 = d.c2; q.c3 = d.c3;
 }
 
 template <int PK>
-__device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const gexs_job& J)
+__device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const gexs_job& J,
+                                         const Tile&)
 {
     q.nu = d.nu; q.invw = d.invw; q.y = d.y;
     q.amp = (PK == PK_ERF) ? d.S : dmul(d.S, d.invw);
@@ -296,8 +303,7 @@ __device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const 
 /* ------------------------------------------------- per-warp line loops */
 template <int PK, int B>
 __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nrec, int wb,
-                                          int lane, const float (&lk)[B], float (&part)[B],
-                                          int erf_form)
+                                          int lane, const float (&lk)[B], float (&part)[B])
 {
     const float wbf = (float)wb;
     for (int i = 0; i < nrec; ++i) {
@@ -309,7 +315,7 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
         const int c1a = lo16(q.c1), c1b = hi16(q.c1);
         if constexpr (PK == PK_VOIGT) {
             const bool far = (c1a >= c1b) || (c1b <= wb) || (c1a >= wb + 32 * B);
-            if (full && far) {
+            if (full && far && !q.wide) {
                 /* every bin of the warp is in region I and in the window */
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
@@ -330,8 +336,13 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
                     if (t < c1a || t >= c1b) {
                         float x2 = x * x;
                         float num = x2 + q.p;
-                        float den = fmaf(x2, -2.f, num * num);
-                        v = num * rcp_approx(den) * q.a1;
+                        if (!q.wide) {
+                            float den = fmaf(x2, -2.f, num * num);
+                            v = num * rcp_approx(den) * q.a1;
+                        } else {
+                            /* num/den = 1/(num - 2 x^2/num) without num^2 */
+                            v = (x < 1e18f) ? q.a1 / (num - 2.f * (x2 / num)) : 0.f;
+                        }
                     } else {
                         int reg;
                         if (t < lo16(c2) || t >= hi16(c2)) reg = 2;
@@ -349,7 +360,9 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
                 const int t = wb + lane + 32 * k;
                 if (t < a || t >= b || t < c1a || t >= c1b) continue;
                 float xd = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
-                part[k] = fmaf(q.amp, erf_bin_f32(xd - q.y, xd + q.y, erf_form), part[k]);
+                /* FP32 always takes the cancellation-free form: the literal
+                 * erf difference loses ~1e-7 absolute in FP32 far wings */
+                part[k] = fmaf(q.amp, erf_bin_f32(xd - q.y, xd + q.y, GEXS_ERF_STABLE), part[k]);
             }
         } else {
             constexpr int NODES = (PK == PK_GH16) ? 16 : 32;
@@ -358,7 +371,8 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
                 const int t = wb + lane + 32 * k;
                 if (!full && (t < a || t >= b)) continue;
                 float x = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
-                part[k] = fmaf(q.a1, gh_sum_f32<NODES>(x, q.p), part[k]);
+                float g = q.wide ? gh_sum_f32_wide<NODES>(x, q.p) : gh_sum_f32<NODES>(x, q.p);
+                part[k] = fmaf(q.a1, g, part[k]);
             }
         }
     }
@@ -515,14 +529,14 @@ tile_kernel(const KArgs args)
                 else { L.gam = 0.0; L.nexp = 0.0; }
                 Derived<PK> d = derive_line<PK>(T, L, zthr);
                 Rec r;
-                make_rec<PK>(r, d, J);
+                make_rec<PK>(r, d, J, T);
                 s_rec[tid] = r;
             }
             __syncthreads();
             issue(s + 2);
 
             if constexpr (PREC == GEXS_FP32) {
-                lines_f32<PK, B>(s_rec, nrec, wb, lane, lk, part, J.erf_form);
+                lines_f32<PK, B>(s_rec, nrec, wb, lane, lk, part);
 #pragma unroll
                 for (int k = 0; k < B; ++k) { kahan_add(ks[k], kc[k], part[k]); part[k] = 0.f; }
             } else {

@@ -57,7 +57,8 @@ extern "C" {
 #define GEXS_WINDOW_ROUNDED   1 /* [round((nu0-cut-f_0)/dnu), round((nu0+cut-f_0)/dnu))
                                    as Managers/CPU/OpenMPManager.cpp:399-400    */
 
-/* form of the bin-averaged erf difference (Doppler, Gaussian) */
+/* form of the bin-averaged erf difference (Doppler, Gaussian) in the FP64
+ * form; the FP32 form always evaluates the stable form */
 #define GEXS_ERF_STABLE   0 /* erfc(xm)-erfc(xp) when xm>=0: no cancellation  */
 #define GEXS_ERF_LITERAL  1 /* erf(xp)-erf(xm) exactly as the reference       */
 
