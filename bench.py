@@ -1,0 +1,469 @@
+#!/usr/bin/env python
+"""Cross-section benchmark: Voigt line-profile evaluations per second.
+
+Workload (one step = one cross-section): the Voigt form of the 1e8-line
+configuration - 2e5 synthetic states (J 0-80), 1e8 transitions with nu0 in
+[100, 30000] cm^-1, pressure broadening gamma_ref ~ U(0.03, 0.1), n ~
+U(0.4, 0.8), T_ref 296 K; T = 1500 K, P = 1 bar, 18 amu; grid 100-30000
+cm^-1 at 0.01 (2,990,001 points), cutoff 25 cm^-1; FP32 profile
+arithmetic with FP64 centres, S(T), Q(T) and Kahan-compensated bins.
+
+value  = line-profile evaluations / s over all ranks (the exact count of
+         (line, bin) pairs inside the cutoff window), device time of the
+         tile kernel with inputs resident in HBM (4.4 GB of lines > L2);
+e2e    = the same through the drop-in manager's C ABI (gexs_manager_*):
+         host->device copy of the line list and the grid seed from pinned
+         memory, the launch, and the device->host read of the result;
+also   = plain FP64 per-(T,P) GPU path on the same workload, the 64-pair
+         uneven-grid batch (FP32, one persistent launch replayed from a CUDA
+         graph) against the plain FP64 path pair by pair, roofline, the
+         reference's own CPU path timed on a bounded sample.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Voigt line-evals/s @1e8 lines; 64-(T,P) batch vs plain FP64; serve p50/p99"
+UNIT = "line-evals/s"
+T_K, P_BAR, MASS, CUT = 1500.0, 1.0, 18.0, 25.0
+NU0, NU1, DNU = 100.0, 30000.0, 0.01
+# Humlicek FLOP per evaluation by region (complex mul 6, add 2, Re-only
+# division 7 + 1 divide, Horner step 7; divide, exp and cos count 1 each)
+FLOPS_REGION = [15.0, 29.0, 71.0, 113.0]
+
+
+def grid_points():
+    return int(round((NU1 - NU0) / DNU)) + 1
+
+
+def world():
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_id):
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", dev_id], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def device_id_for_smi(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        return ids[dev] if dev < len(ids) else str(dev)
+
+
+# --------------------------------------------------------- CPU baseline
+def cpu_reference_sample(target_s=12.0, seed_states=1002, seed_lines=2002):
+    """Reference CPU path (OpenMPManager::ComputeVoigtTP + humlic, compiled
+    from the reference sources at -O3 -march=x86-64-v3) on a bounded sample
+    of the Voigt workload's distribution, all host threads.  Returns
+    (evals/s, threads, sample description, kind)."""
+    from gexs_b200 import synth
+    from oracle import pyoracle as po
+    from gexs_b200 import _capi as capi
+    from gexs_b200.engine import job_init
+    from tests.helpers import host_job
+    kind = "reference" if po.ref_available(fast=True) else "port"
+    threads = len(os.sched_getaffinity(0))
+    st = synth.make_states(200000, 80, seed_states)
+    L = synth.make_lines(st, 2000000, NU0, NU1, seed_lines, broadening_seed=seed_lines + 1000)
+    q = po.partition(st.energy, st.g, T_K)
+
+    def run(k):
+        mid = len(L["nu"]) // 2
+        sl = slice(mid - k // 2, mid - k // 2 + k)
+        S = {kk: np.ascontiguousarray(v[sl]) for kk, v in L.items()}
+        lo = S["nu"][0] - CUT - 1.0
+        nb = int((S["nu"][-1] + CUT + 1.0 - lo) / DNU) + 1
+        freq = lo + np.arange(nb, dtype=np.float64) * DNU
+        j = job_init(capi.CONV_REF_CPU, capi.VOIGT, T_K, P_BAR, q, MASS, lo, DNU, nb,
+                     ref_temp=296.0)
+        ev = po.count_evals(host_job(j, S))
+        t0 = time.perf_counter()
+        if kind == "reference":
+            po.ref_voigt_tp(freq, S, T_K, P_BAR, q, MASS, 296.0, DNU, nthreads=threads, fast=True)
+        else:
+            po.cross_section(host_job(j, S), nthreads=threads)
+        return ev, time.perf_counter() - t0
+
+    k = 2000
+    ev, dt = run(k)
+    while dt < 0.5 and k < len(L["nu"]) // 2:
+        k *= 4
+        ev, dt = run(k)
+    rate = ev / dt
+    k = int(min(len(L["nu"]) - 2, k * max(1.0, target_s / max(dt, 1e-3))))
+    ev, dt = run(k)
+    sample = ("%d consecutive lines around the median nu0 of a 2e6-line list with the "
+              "workload's distribution; %.3g evaluations in %.1f s (reference CPU "
+              "conventions: HWHM Doppler scaling, cutoff min(25P,100)=25)" % (k, ev, dt))
+    return ev / dt, threads, sample, kind
+
+
+def reference_arm(args):
+    ws, rank, _ = world()
+    if rank != 0:
+        return 0
+    try:
+        from oracle import pyoracle as po
+        if not os.path.exists(po.ORACLE_LIB):
+            po.build(with_reference=False)
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": "CPU checker build failed: %s" % e}))
+        return 0
+    rates = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        r, threads, sample, kind = cpu_reference_sample(target_s=args.cpu_seconds)
+        info = (threads, sample, kind)
+        if i >= args.warmup:
+            rates.append(r)
+    value = float(np.mean(rates))
+    evals_per_step = value * args.cpu_seconds
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * args.cpu_seconds, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Voigt, 1e8-line list distribution, T=1500 K, P=1 bar, "
+                                   "0.01 cm^-1 grid, cutoff 25 (bounded CPU sample per step)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[0], "kind": info[2],
+                             "sample": info[1]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "evals_per_step": evals_per_step}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- our arm
+def region_flops(L, q):
+    """FLOP per evaluation from the oracle's region histogram on a sample of
+    8000 lines (uniform in line index) on the full grid."""
+    from gexs_b200 import _capi as capi
+    from gexs_b200.engine import job_init
+    from oracle import pyoracle as po
+    from tests.helpers import host_job
+    n = L["nu"].shape[0]
+    idx = np.linspace(0, n - 1, 8000).astype(np.int64)
+    import torch
+    ti = torch.as_tensor(idx, device=L["nu"].device)
+    S = {k: np.ascontiguousarray(v[ti].cpu().numpy()) for k, v in L.items()}
+    j = job_init(capi.CONV_PHYSICAL, capi.VOIGT, T_K, P_BAR, q, MASS, NU0, DNU, grid_points(),
+                 cutoff=CUT)
+    hist = np.array(po.region_hist(host_job(j, S)), dtype=np.float64)
+    frac = hist / hist.sum()
+    return float(np.dot(frac, FLOPS_REGION)), [float(f) for f in frac]
+
+
+def batch64(ctx, torch, dev):
+    """The 64-(T,P) uneven-grid batch over the 1e6-line list: FP32 batched
+    (autotuned, graph-replayed persistent launch) vs plain FP64 per pair."""
+    from gexs_b200 import synth, _capi as capi
+    from gexs_b200.engine import Job, LineList
+    st = synth.make_states(20000, 40, 1001)
+    L = synth.make_lines(st, 1000000, NU0, 10000.0, 2001, broadening_seed=3001)
+    lines = LineList.from_dict(L, device=dev)
+    se = torch.as_tensor(st.energy, device=dev)
+    sg = torch.as_tensor(st.g, device=dev)
+    temps = np.logspace(np.log10(100.0), np.log10(3000.0), 8)
+    press = np.logspace(-5.0, 2.0, 8)
+    rng = np.random.Generator(np.random.PCG64(4003))
+    dnus = rng.choice([0.1, 0.01, 0.005], size=64)
+    qs = ctx.partition(se, sg, np.repeat(temps, 8))
+    j32, j64 = [], []
+    for i in range(64):
+        T, P, d = temps[i // 8], press[i % 8], float(dnus[i])
+        G = int(round((30000.0 - NU0) / d)) + 1
+        kw = dict(convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=T, pressure=P,
+                  partition=float(qs[i]), mass=MASS, nu_start=NU0, dnu=d, grid_points=G,
+                  cutoff=CUT)
+        j32.append(Job(lines, torch.zeros(G, dtype=torch.float64, device=dev),
+                       precision=capi.FP32, **kw))
+        j64.append(Job(lines, torch.zeros(G, dtype=torch.float64, device=dev),
+                       precision=capi.FP64, **kw))
+    evals = sum(ctx.count_evals(j32))
+    cfg, tune_ms = ctx.autotune(j32)
+    b = ctx.batch(j32, cfg)
+    s = torch.cuda.Stream(device=dev)
+    b.capture(s)
+    b.replay(s)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t32 = []
+    for _ in range(2):
+        e0.record(s); b.replay(s); e1.record(s); e1.synchronize()
+        t32.append(e0.elapsed_time(e1))
+    ctx.check(s)
+    cur = torch.cuda.current_stream(dev)
+    ctx.run(j64[:1])
+    ctx.check()
+    e0.record(cur)
+    for j in j64:
+        ctx.run([j], stream=cur)
+    e1.record(cur)
+    e1.synchronize()
+    ctx.check()
+    t64 = e0.elapsed_time(e1)
+    worst, band = 0.0, 0.0
+    for a, c in zip(j32, j64):
+        x, r = a.out, c.out
+        pk = float(r.max())
+        if pk <= 0:
+            continue
+        m = r > 1e-6 * pk
+        worst = max(worst, float(((x[m] - r[m]).abs() / r[m]).max()))
+        band = max(band, abs(float(x.sum()) - float(r.sum())) / float(r.sum()))
+    b.close()
+    return {"pairs": 64, "lines": lines.count, "evals": evals,
+            "fp32_batched_ms": min(t32), "fp64_plain_ms": t64, "speedup": t64 / min(t32),
+            "fp32_evals_per_s": evals / (min(t32) * 1e-3),
+            "max_rel_err_vs_fp64": worst, "max_band_err_vs_fp64": band,
+            "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]},
+            "grids": {"0.1": int(np.sum(dnus == 0.1)), "0.01": int(np.sum(dnus == 0.01)),
+                      "0.005": int(np.sum(dnus == 0.005))}}
+
+
+def e2e_manager(torch, dev, L, q, steps, warmup, local_rank):
+    """Same workload through the drop-in manager's C ABI with host buffers."""
+    from gexs_b200 import _capi as capi
+    from gexs_b200.engine import Manager
+    G = grid_points()
+    n = int(L["nu"].shape[0])
+    pin = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in L.items()}
+    for k in pin:
+        pin[k].copy_(L[k])
+    h = {k: v.numpy() for k, v in pin.items()}
+    freq = NU0 + np.arange(G, dtype=np.float64) * DNU
+    zeros = torch.zeros(G, dtype=torch.float64, pin_memory=True).numpy()
+    res = torch.zeros(G, dtype=torch.float64, pin_memory=True).numpy()
+    lb = sum(v.numel() * v.element_size() for v in pin.values())
+    m = Manager(capi.VOIGT, device=local_rank, convention=capi.CONV_PHYSICAL, precision=capi.FP32,
+                memory_bytes=lb + 2 * G * 8 + (256 << 20))
+    m.initialize_vectors(G, 1)
+    m.initialize_constants(0.0, T_K, q, DNU, MASS, P_BAR, 296.0, 1.0)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        m.transfer_freq(freq, zeros)
+        m.transfer_vectors(h["elow"], h["nu"], h["aif"], h["gns"], h["gamma"], h["n"])
+        m.execute(G, n, 0, T_K, P_BAR, q)
+        m.transfer_results(freq, res, 0)
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    m.close()
+    return float(np.sum(times)), lb + G * 8, G * 8, res.copy()
+
+
+def our_arm(args):
+    import torch
+    ws, rank, local_rank = world()
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = "cuda:%d" % local_rank
+    torch.cuda.set_device(local_rank)
+    from gexs_b200 import Context, Job, LineList, synth, _capi as capi
+    from oracle import pyoracle as po
+    if not os.path.exists(po.ORACLE_LIB):
+        po.build(with_reference=False)
+
+    st = synth.make_states(200000, 80, 1002)
+    L = synth.make_lines_torch(st, args.lines, NU0, NU1, 2002, broadening_seed=3002, device=dev)
+    lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev)
+    q = po.partition(st.energy, st.g, T_K)
+    G = grid_points()
+    out = torch.zeros(G, dtype=torch.float64, device=dev)
+    ctx = Context(local_rank)
+    job = Job(lines, out, convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=T_K,
+              pressure=P_BAR, partition=q, mass=MASS, nu_start=NU0, dnu=DNU, grid_points=G,
+              precision=capi.FP32, cutoff=CUT)
+    evals = ctx.count_evals([job])[0]
+    cfg, _ = ctx.autotune([job]) if args.autotune else ((4, 4, 0), 0.0)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        ctx.run([job], cfg=cfg, stream=stream)
+    ctx.check(stream)
+    sampler = ClockSampler(device_id_for_smi(torch, local_rank))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.run([job], cfg=cfg, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ctx.check(stream)
+    ms = e0.elapsed_time(e1)
+    tmax = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    ms_max = float(tmax.item())
+    value = evals * args.steps * ws / (ms_max * 1e-3)
+    launch_ms = ms / args.steps
+
+    # plain FP64 per-(T,P) path on the same workload
+    out64 = torch.zeros(G, dtype=torch.float64, device=dev)
+    j64 = Job(lines, out64, convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=T_K,
+              pressure=P_BAR, partition=q, mass=MASS, nu_start=NU0, dnu=DNU, grid_points=G,
+              precision=capi.FP64, cutoff=CUT)
+    ctx.run([j64], stream=stream)
+    ctx.check(stream)
+    e0.record(stream); ctx.run([j64], stream=stream); e1.record(stream); e1.synchronize()
+    fp64_ms = e0.elapsed_time(e1)
+    pk = float(out64.max())
+    msk = out64 > 1e-6 * pk
+    fp32_err = float(((out[msk] - out64[msk]).abs() / out64[msk]).max())
+    band_err = abs(float(out.sum()) - float(out64.sum())) / float(out64.sum())
+    integral = float(out64.sum()) * DNU
+    del out64, j64
+
+    # e2e through the manager C ABI, host buffers
+    e2e_s, h2d, d2h, e2e_res = e2e_manager(torch, dev, L, q, args.steps, min(args.warmup, 1),
+                                           local_rank)
+    e2e_match = float(np.max(np.abs(e2e_res - out.cpu().numpy())) / max(pk, 1e-300))
+    tmax2 = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(tmax2, op=dist.ReduceOp.MAX)
+    e2e_value = evals * args.steps * ws / float(tmax2.item())
+
+    result = None
+    if rank == 0:
+        peak = 0.0
+        import ctypes as C
+        from gexs_b200._capi import lib
+        pv = C.c_double()
+        if lib().gexs_probe_fp32_tflops(local_rank, C.byref(pv)) == 0:
+            peak = pv.value
+        fpe, frac = region_flops(L, q)
+        achieved = evals * fpe / (launch_ms * 1e-3) / 1e12
+        line_bytes = lines.nbytes()
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic_voigt_fp32.json")
+        if os.path.exists(tp):
+            try:
+                traffic = json.load(open(tp)).get("bytes_per_launch_scaled")
+            except Exception:
+                traffic = None
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "Voigt FP32-profile cross-section, 1e8-line synthetic list "
+                                   "(2e5 states, J 0-80, nu0 100-30000), T=1500 K, P=1 bar, "
+                                   "grid 100-30000 @0.01 (2,990,001 pts), cutoff 25",
+                       "lines": lines.count, "grid_points": G, "evals_per_step": evals,
+                       "per_rank": "one full cross-section per rank",
+                       "l2": "inputs (%.1f GB of lines) larger than L2" % (line_bytes / 1e9),
+                       "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]}},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "traffic": traffic,
+                         "peak_source": "measured FP32 FMA rate of this GPU "
+                                        "(gexs_probe_fp32_tflops); MEASURED_PEAKS.json has "
+                                        "no FP32 figure",
+                         "flop_per_eval": fpe, "region_fractions": frac,
+                         "launch_ms": launch_ms,
+                         "line_stream_gbs": line_bytes / (launch_ms * 1e-3) / 1e9},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "path": "gexs_manager_* C ABI, pinned host",
+                    "max_abs_diff_vs_device_run_over_peak": e2e_match},
+            "fp64_plain": {"ms": fp64_ms, "evals_per_s": evals / (fp64_ms * 1e-3),
+                           "fp32_speedup": fp64_ms / launch_ms},
+            "accuracy": {"fp32_max_rel_vs_fp64_bins_gt_1e-6_peak": fp32_err,
+                         "fp32_band_rel_vs_fp64": band_err, "integrated_fp64": integral},
+            "clocks": clocks,
+        }
+    if not args.no_batch and rank == 0:
+        result["batch64"] = batch64(ctx, torch, dev)
+    if not args.no_cpu and rank == 0 and ws == 1:
+        v, cores, sample, kind = cpu_reference_sample(target_s=args.cpu_seconds)
+        result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                                  "sample": sample}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--lines", type=int, default=100_000_000)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -68,6 +68,7 @@ SIGNATURES = [
                                 C.POINTER(GexsLaunchCfg), C.POINTER(C.c_float)]),
     ("gexs_partition", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
+    ("gexs_probe_fp32_tflops", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     ("gexs_manager_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
                                       C.POINTER(C.c_void_p)]),
     ("gexs_manager_destroy", C.c_int, [C.c_void_p]),

@@ -20,6 +20,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
 SOURCES = [
     "csrc/gexs_kernels.cu",
     "csrc/gexs_capi.cu",
+    "csrc/gexs_calib.cu",
     "host/B200Manager.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")

@@ -204,6 +204,13 @@ int gexs_partition(gexs_ctx* ctx, const double* d_energy, const int32_t* d_g,
                    int64_t nstates, const double* h_temps, int nt,
                    double* h_q);
 
+/* ------------------------------------------------------------ calibration
+ * Measured FP32 FMA throughput of `device` in TFLOP/s (2 FLOP per FMA):
+ * the roofline denominator of the FP32-profile kernels, which are bound by
+ * FP32/SFU issue rather than HBM or tensor cores.  No reference
+ * counterpart. */
+int gexs_probe_fp32_tflops(int device, double* tflops);
+
 /* ------------------------------------------------------------ manager ABI
  * Flat C view of the drop-in manager (B200Manager, a BaseManager subclass):
  * one function per BaseManager virtual (Managers/BaseManager.h:22-35) so an
