@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(_HERE, "libgexs_b200.so")
 
 GEXS_OK = 0
 GEXS_ERR_NOT_READY = -5
+NOALLOC_MAX_JOBS = 64
 
 GAUSSIAN, DOPPLER, VOIGT, VOIGT_QUAD = 0, 1, 2, 4
 FP64, FP32 = 0, 1
@@ -54,6 +55,8 @@ SIGNATURES = [
     ("gexs_ctx_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     ("gexs_ctx_destroy", C.c_int, [C.c_void_p]),
     ("gexs_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("gexs_run_noalloc", C.c_int, [C.POINTER(GexsJob), C.c_int, C.POINTER(GexsLaunchCfg),
+                                   C.c_void_p]),
     ("gexs_run", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
                            C.POINTER(GexsLaunchCfg), C.c_void_p]),
     ("gexs_count_evals", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,

@@ -21,6 +21,7 @@ SOURCES = [
     "csrc/gexs_kernels.cu",
     "csrc/gexs_capi.cu",
     "csrc/gexs_calib.cu",
+    "csrc/gexs_noalloc.cu",
     "host/B200Manager.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")

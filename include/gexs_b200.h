@@ -177,6 +177,32 @@ int gexs_ctx_check(gexs_ctx* ctx, void* stream);
 int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
                      int64_t* h_counts);
 
+/* --------------------------------------------- run without allocating
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory while they run: for instance a plug-in inside a host
+ * program that keeps all of the GPU's memory in its own pool, or a
+ * latency-sensitive loop in which a device allocation could stall other
+ * streams or fail.  gexs_run takes its launch tables and work counter from
+ * cudaMallocAsync; this variant keeps them in a fixed array inside the
+ * library's device image (GEXS_NOALLOC_SCRATCH_BYTES on every GPU that
+ * loads the library, held until the process exits) and calls no
+ * cudaMalloc, cudaFree or other allocating routine.
+ *  - The caller still provides the line arrays and the output grids.
+ *  - At most GEXS_NOALLOC_MAX_JOBS jobs per call, all of one profile class
+ *    and precision; larger or mixed calls return GEXS_ERR_INVALID.
+ *  - Runs on the calling thread's current device.  The first call on a
+ *    device looks up the array's device address (cudaGetSymbolAddress);
+ *    make that first call before any stream capture on that device.
+ *  - Every call on a device shares the one array and it keeps the last
+ *    call's contents (the work counter is reset by each call): calls whose
+ *    work overlaps on the GPU, from any stream or thread, race and must be
+ *    serialised by the caller.
+ * cfg NULL = 4 bins per lane, 8 warps. */
+#define GEXS_NOALLOC_MAX_JOBS      64
+#define GEXS_NOALLOC_SCRATCH_BYTES 16384
+int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
+                     void* stream);
+
 /* ------------------------------------------------------ batched launches
  * A batch owns its device job table and work-item table; launching it is
  * one memset of the work counter plus one persistent kernel, which can be
