@@ -331,7 +331,8 @@ def our_arm(args):
               pressure=P_BAR, partition=q, mass=MASS, nu_start=NU0, dnu=DNU, grid_points=G,
               precision=capi.FP32, cutoff=CUT)
     evals = ctx.count_evals([job])[0]
-    cfg, _ = ctx.autotune([job]) if args.autotune else ((4, 4, 0), 0.0)
+    cfg, _ = ctx.autotune([job]) if args.autotune else \
+        (tuple(int(v) for v in args.cfg.split(",")), 0.0)
     stream = torch.cuda.current_stream(dev)
 
     for _ in range(args.warmup):
@@ -456,6 +457,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--cfg", default="4,4,0",
+                    help="launch shape bins_per_lane,warps,ctas_per_sm of the timed kernel")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -29,30 +29,42 @@
 
 namespace gexs {
 
-/* --------------------------------------------------------------- records */
-struct RecF32 {            /* 48 bytes */
+/* --------------------------------------------------------------- records
+ * One derived record per (line, tile), written by the thread that derived
+ * the line and read by every warp as 16-byte broadcast loads. */
+struct __align__(16) RecF32 {   /* 48 bytes */
     float icf;             /* tile-relative centre bin floor(tc), exact      */
-    float dx;              /* dnu * invw                                     */
+    float dx;              /* dnu * invw: x per bin                          */
     float mfcdx;           /* -(tc - floor(tc)) * dx                         */
     float a1;              /* Voigt: amp*0.5641896*y ; GH: amp*y/pi          */
     float p;               /* Voigt: 0.5 + y^2 ; GH: y^2                     */
     float y;               /* Voigt/GH: y ; Doppler: half bin in x units     */
     float amp;             /* Voigt/GH: S*invw*out_scale ; Doppler: S*out    */
-    int   wide;            /* 1: |x| may exceed 1e8 in this tile; use the
-                              overflow-free forms                            */
+    float fc;              /* tc - floor(tc) in [0, 1)                       */
     int   win;             /* a | b << 16 : bins [a, b) of the tile          */
-    int   c1;              /* Voigt: bins not in region I ; Doppler: bins
-                              whose xm <= zero threshold                     */
-    int   c2;              /* Voigt: bins in regions III/IV                  */
-    int   c3;              /* Voigt: bins satisfying the region-III test     */
+    int   c1;              /* Voigt: bins not in region I (the core) ;
+                              Doppler: bins whose xm <= the zero threshold   */
+    int   mask;            /* per warp w: bit w touches, bit 8+w fast tier,
+                              bit 16+w mid tier; bit 24: |x| may exceed 1e8
+                              in this tile (overflow-free forms)             */
+    int   pad;
 };
 
-struct RecF64 {            /* 48 bytes */
+struct __align__(16) RecF64 {   /* 64 bytes */
     double nu;             /* centre after the nu==0 rule                   */
     double invw;
     double y;              /* Voigt/GH: y ; Doppler: unused                 */
-    double amp;            /* Voigt/GH: S*invw*out_scale ; Doppler: S*out   */
+    double amp;            /* Voigt/GH: S*invw ; Doppler: S                 */
     int    win, c1, c2, c3;
+    int    mask, pad0, pad1, pad2;
+};
+
+/* FP64 view of a line for its core (Humlicek regions II-IV), which the
+ * FP32 form evaluates in a separate pass */
+struct CoreF64 {
+    double nu, invw, y, amp;
+    int c2;                /* bins in regions III/IV                        */
+    int c3;                /* bins satisfying the region-III test           */
 };
 
 template <int PREC> struct RecOf;
@@ -65,6 +77,9 @@ __device__ __forceinline__ int hi16(int v) { return (int)((unsigned)v >> 16); }
 
 /* profile classes of the kernel template */
 enum { PK_VOIGT = 0, PK_ERF = 1, PK_GH16 = 2, PK_GH32 = 3 };
+
+/* lines derived per thread between two CTA barriers */
+constexpr int PH = 2;
 
 /* ------------------------------------------------------- cp.async helpers */
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
@@ -185,7 +200,7 @@ struct Derived {
 };
 
 template <int PK>
-__device__ __forceinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L, double zthr)
+__device__ __noinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L, double zthr)
 {
     const gexs_job& J = *T.J;
     Derived<PK> d;
@@ -257,8 +272,35 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
     s = t;
 }
 
+/* per-warp tiers of a line (bits of RecF*.mask).  Warp w owns bins
+ * [32*B*w, 32*B*(w+1)) of the tile. */
+template <int PK, int B, int WARPS>
+__device__ __forceinline__ int warp_mask(const Derived<PK>& d, int wide)
+{
+    const int a = lo16(d.win), b = hi16(d.win);
+    const int c1a = lo16(d.c1), c1b = hi16(d.c1);
+    const int ic = (int)fmin(fmax(floor(d.tc), -1e6), 1e6);
+    int m = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        const int r0 = 32 * B * w, r1 = r0 + 32 * B;
+        bool touch = a < r1 && b > r0;
+        if (PK == PK_ERF) touch = touch && c1a < r1 && c1b > r0 && c1a < c1b;
+        if (!touch) continue;
+        m |= 1 << w;
+        if (PK == PK_ERF || wide) continue;
+        const bool full = a <= r0 && b >= r1;
+        const bool coredisj = (PK != PK_VOIGT) || c1a >= c1b || c1b <= r0 || c1a >= r1;
+        /* the single-FMA x of the fast tier keeps ~1e-7 relative accuracy
+         * only when the centre is at least a warp span away */
+        const bool far = ic < r0 - 32 * B || ic > r1 + 32 * B;
+        if (full && coredisj) m |= 1 << (far ? 8 + w : 16 + w);
+    }
+    return m | (wide << 24);
+}
+
 /* --------------------------------------------------------- record builders */
-template <int PK>
+template <int PK, int B, int WARPS>
 __device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const gexs_job& J,
                                          const Tile& T)
 {
@@ -283,111 +325,194 @@ __device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const 
         q.p = (float)(d.y * d.y);
         q.y = (float)d.y;
     }
-    {
-        /* largest |x| the line reaches in this tile */
-        double dfar = fmax(fabs(d.nu - T.f0), fabs(d.nu - T.fl));
-        q.wide = (dfar * d.invw > 1e8) ? 1 : 0;
-    }
-    q.win = d.win; q.c1 = d.c1; q.c2 = d.c2; q.c3 = d.c3;
+    q.fc = fc;
+    q.win = d.win; q.c1 = d.c1;
+    /* largest |x| the line reaches in this tile */
+    double dfar = fmax(fabs(d.nu - T.f0), fabs(d.nu - T.fl));
+    const int wide = (dfar * d.invw > 1e8) ? 1 : 0;
+    q.mask = (d.win == 0) ? 0 : warp_mask<PK, B, WARPS>(d, wide);
+    q.pad = 0;
 }
 
-template <int PK>
-__device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const gexs_job& J,
+template <int PK, int B, int WARPS>
+__device__ __forceinline__ void make_rec(RecF64& q, const Derived<PK>& d, const gexs_job&,
                                          const Tile&)
 {
     q.nu = d.nu; q.invw = d.invw; q.y = d.y;
     q.amp = (PK == PK_ERF) ? d.S : dmul(d.S, d.invw);
     q.win = d.win; q.c1 = d.c1; q.c2 = d.c2; q.c3 = d.c3;
+    q.mask = (d.win == 0) ? 0 : warp_mask<PK, B, WARPS>(d, 1);
+    q.pad0 = q.pad1 = q.pad2 = 0;
 }
 
-/* ------------------------------------------------- per-warp line loops */
-template <int PK, int B>
-__device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nrec, int wb,
-                                          int lane, const float (&lk)[B], float (&part)[B])
+/* FP64 Humlicek for a core bin of the FP32 form, kept out of line so the
+ * FP32 loop does not carry its registers */
+__device__ __noinline__ float core_term_f64(int reg, double f, const CoreF64& cd)
 {
-    const float wbf = (float)wb;
+    const double xd = dmul(fabs(dsub(f, cd.nu)), cd.invw);
+    return (float)(cd.amp * hum_by_region<double>(reg, xd, cd.y));
+}
+
+/* ------------------------------------------------- per-warp line loops
+ * FP32 form.  Lane l of warp w owns bins t_k = wb + l + 32k (k < B).
+ * fast tier: whole warp in the window, in region I, centre >= one warp
+ *   span away: x_k = fma(32k, dx, fma(l, dx, q)) and the region-I closed
+ *   form, 7 issue slots + 1 MUFU per bin;
+ * mid tier: as fast but the centre is near: x = ((l+32k + wb-ic) - fc)*dx
+ *   exactly, so bins next to the centre keep full relative accuracy;
+ * general: per-bin window and region tests; Humlicek regions II-IV (the
+ *   line core, which carries most of its area) in FP64. */
+template <int PK, int B>
+__device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec,
+                                          const CoreF64* __restrict__ core, int nrec, int warp,
+                                          int lane, float (&part)[B], double nu_start, double dnu,
+                                          int64_t j0)
+{
+    const int wb = warp * 32 * B;
+    const float wbf = (float)wb, lanef = (float)lane;
+    const int bit = 1 << warp;
     for (int i = 0; i < nrec; ++i) {
-        const RecF32& q = rec[i];
-        const int a = lo16(q.win), b = hi16(q.win);
-        if (b <= wb || a >= wb + 32 * B) continue;
-        const bool full = (a <= wb) && (b >= wb + 32 * B);
-        const float ncf = wbf - q.icf;
-        const int c1a = lo16(q.c1), c1b = hi16(q.c1);
+        const int4 qi = *reinterpret_cast<const int4*>(&rec[i].win);   /* win c1 mask pad */
+        const int mask = qi.z;
+        if (!(mask & bit)) continue;
+        const float4 q0 = *reinterpret_cast<const float4*>(&rec[i].icf);   /* icf dx mfcdx a1 */
+        const float4 q1 = *reinterpret_cast<const float4*>(&rec[i].p);     /* p y amp fc */
+        const float ncf = wbf - q0.x;
         if constexpr (PK == PK_VOIGT) {
-            const bool far = (c1a >= c1b) || (c1b <= wb) || (c1a >= wb + 32 * B);
-            if (full && far && !q.wide) {
-                /* every bin of the warp is in region I and in the window */
+            if (mask & (bit << 8)) {
+                const float x0 = fmaf(lanef, q0.y, fmaf(ncf, q0.y, q0.z));
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
-                    float x = fmaf(lk[k] + ncf, q.dx, q.mfcdx);
-                    float x2 = x * x;
-                    float num = x2 + q.p;
-                    float den = fmaf(x2, -2.f, num * num);
-                    part[k] = fmaf(num * rcp_approx(den), q.a1, part[k]);
+                    const float x = fmaf((float)(32 * k), q0.y, x0);
+                    const float x2 = x * x;
+                    const float num = x2 + q1.x;
+                    const float den = fmaf(x2, -2.f, num * num);
+                    part[k] = fmaf(num * rcp_approx(den), q0.w, part[k]);
                 }
-            } else {
-                const int c2 = q.c2, c3 = q.c3;
+                continue;
+            }
+            const float t0 = lanef + ncf;   /* exact: small integers */
+            if (mask & (bit << 16)) {
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
-                    const int t = wb + lane + 32 * k;
-                    if (t < a || t >= b) continue;
-                    float x = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
-                    float v;
-                    if (t < c1a || t >= c1b) {
-                        float x2 = x * x;
-                        float num = x2 + q.p;
-                        if (!q.wide) {
-                            float den = fmaf(x2, -2.f, num * num);
-                            v = num * rcp_approx(den) * q.a1;
-                        } else {
-                            /* num/den = 1/(num - 2 x^2/num) without num^2 */
-                            v = (x < 1e18f) ? q.a1 / (num - 2.f * (x2 / num)) : 0.f;
-                        }
-                    } else {
-                        int reg;
-                        if (t < lo16(c2) || t >= hi16(c2)) reg = 2;
-                        else reg = (t >= lo16(c3) && t < hi16(c3)) ? 3 : 4;
-                        v = q.amp * hum_by_region<float>(reg, x, q.y);
-                    }
-                    part[k] += v;
+                    const float x = ((t0 + (float)(32 * k)) - q1.w) * q0.y;
+                    const float x2 = x * x;
+                    const float num = x2 + q1.x;
+                    const float den = fmaf(x2, -2.f, num * num);
+                    part[k] = fmaf(num * rcp_approx(den), q0.w, part[k]);
                 }
+                continue;
+            }
+            /* general tier: window edges and region-I bins of warps that
+             * hold part of the core; the core bins themselves are left to
+             * core_pass_f32 */
+            const int a = lo16(qi.x), b = hi16(qi.x);
+            const int c1a = lo16(qi.y), c1b = hi16(qi.y);
+            const bool wide = (mask >> 24) & 1;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = wb + lane + 32 * k;
+                if (t < a || t >= b || (t >= c1a && t < c1b)) continue;
+                const float x = fabsf(((t0 + (float)(32 * k)) - q1.w) * q0.y);
+                const float x2 = x * x;
+                const float num = x2 + q1.x;
+                float v;
+                if (!wide) {
+                    const float den = fmaf(x2, -2.f, num * num);
+                    v = num * rcp_approx(den) * q0.w;
+                } else {
+                    /* num/den = 1/(num - 2 x^2/num) without num^2 */
+                    v = (x < 1e18f) ? q0.w / (num - 2.f * (x2 / num)) : 0.f;
+                }
+                part[k] += v;
             }
         } else if constexpr (PK == PK_ERF) {
-            /* outside [c1a, c1b) every term is an exact zero */
-            if (c1a >= c1b || c1b <= wb || c1a >= wb + 32 * B) continue;
+            const int a = lo16(qi.x), b = hi16(qi.x);
+            const int c1a = lo16(qi.y), c1b = hi16(qi.y);
+            const float t0 = lanef + ncf;
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const int t = wb + lane + 32 * k;
                 if (t < a || t >= b || t < c1a || t >= c1b) continue;
-                float xd = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
+                const float xd = fabsf(((t0 + (float)(32 * k)) - q1.w) * q0.y);
                 /* FP32 always takes the cancellation-free form: the literal
                  * erf difference loses ~1e-7 absolute in FP32 far wings */
-                part[k] = fmaf(q.amp, erf_bin_f32(xd - q.y, xd + q.y, GEXS_ERF_STABLE), part[k]);
+                part[k] = fmaf(q1.z, erf_bin_f32(xd - q1.y, xd + q1.y, GEXS_ERF_STABLE), part[k]);
             }
         } else {
             constexpr int NODES = (PK == PK_GH16) ? 16 : 32;
+            if (mask & (bit << 8)) {
+                const float x0 = fmaf(lanef, q0.y, fmaf(ncf, q0.y, q0.z));
+#pragma unroll
+                for (int k = 0; k < B; ++k)
+                    part[k] = fmaf(q0.w, gh_sum_f32<NODES>(fabsf(fmaf((float)(32 * k), q0.y, x0)), q1.x),
+                                   part[k]);
+                continue;
+            }
+            const int a = lo16(qi.x), b = hi16(qi.x);
+            const bool wide = (mask >> 24) & 1;
+            const float t0 = lanef + ncf;
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const int t = wb + lane + 32 * k;
-                if (!full && (t < a || t >= b)) continue;
-                float x = fabsf(fmaf(lk[k] + ncf, q.dx, q.mfcdx));
-                float g = q.wide ? gh_sum_f32_wide<NODES>(x, q.p) : gh_sum_f32<NODES>(x, q.p);
-                part[k] = fmaf(q.a1, g, part[k]);
+                if (t < a || t >= b) continue;
+                const float x = fabsf(((t0 + (float)(32 * k)) - q1.w) * q0.y);
+                const float g = wide ? gh_sum_f32_wide<NODES>(x, q1.x) : gh_sum_f32<NODES>(x, q1.x);
+                part[k] = fmaf(q0.w, g, part[k]);
             }
         }
     }
 }
 
+/* Core pass of the FP32 Voigt form: the bins of each line's core (not in
+ * Humlicek region I) in this phase.  Lines are dealt to warps round-robin
+ * and a warp's lanes take consecutive core bins, so the FP64 work is spread
+ * evenly over the CTA instead of landing on the warp that owns the bins.
+ * Region II is evaluated in FP32, regions III/IV (where extracting the real
+ * part of a mostly imaginary w(z) amplifies FP32 rounding ~100x) in FP64.
+ * Each warp adds into its own accumulator row: every bin receives its core
+ * terms in a fixed order. */
+template <int WARPS>
+__device__ __forceinline__ void core_pass_f32(const RecF32* __restrict__ rec,
+                                              const CoreF64* __restrict__ core, int nrec,
+                                              int warp, int lane, float* __restrict__ wacc,
+                                              double nu_start, double dnu, int64_t j0)
+{
+    for (int i = warp; i < nrec; i += WARPS) {
+        const int c1 = rec[i].c1;
+        const int c1a = lo16(c1), c1b = hi16(c1);
+        if (c1a >= c1b) continue;
+        const float icf = rec[i].icf, fc = rec[i].fc, dx = rec[i].dx, y = rec[i].y;
+        const float amp = rec[i].amp;
+        const int c2 = core[i].c2, c3 = core[i].c3;
+        for (int t = c1a + lane; t < c1b; t += 32) {
+            float v;
+            if (t < lo16(c2) || t >= hi16(c2)) {
+                const float x = fabsf(((float)t - icf) - fc) * dx;
+                v = amp * hum_region2<float>(x, y);
+            } else {
+                const int reg = (t >= lo16(c3) && t < hi16(c3)) ? 3 : 4;
+                v = core_term_f64(reg, grid_f(nu_start, dnu, j0 + t), core[i]);
+            }
+            wacc[t] += v;
+        }
+    }
+}
+
+/* FP64 form: per-bin window and region tests, FP64 arithmetic, bins sum
+ * their lines in line order (the order of the FP64 oracle). */
 template <int PK, int B>
-__device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nrec, int wb,
+__device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nrec, int warp,
                                           int lane, const double (&fbin)[B], double (&acc)[B],
                                           const gexs_job& J)
 {
+    const int wb = warp * 32 * B;
+    const int bit = 1 << warp;
     const double out_scale = J.out_scale;
     for (int i = 0; i < nrec; ++i) {
         const RecF64& q = rec[i];
+        if (!(q.mask & bit)) continue;
         const int a = lo16(q.win), b = hi16(q.win);
-        if (b <= wb || a >= wb + 32 * B) continue;
         if constexpr (PK == PK_VOIGT) {
             const int c1 = q.c1, c2 = q.c2, c3 = q.c3;
 #pragma unroll
@@ -404,7 +529,6 @@ __device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nr
             }
         } else if constexpr (PK == PK_ERF) {
             const int c1a = lo16(q.c1), c1b = hi16(q.c1);
-            if (c1a >= c1b || c1b <= wb || c1a >= wb + 32 * B) continue;
             const int form = J.erf_form;
             const double h = 0.5 * J.dnu;
 #pragma unroll
@@ -432,28 +556,57 @@ __device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nr
     }
 }
 
-/* ---------------------------------------------------------------- kernel */
+/* shared-memory layout of one CTA (dynamic shared memory) */
 template <int PK, int PREC, int B, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+struct Smem {
+    static constexpr int NT = WARPS * 32;
+    static constexpr int W = 32 * B * WARPS;
+    static constexpr int R = PH * NT;                       /* lines per phase */
+    static constexpr bool PRESS = (PK != PK_ERF);
+    static constexpr bool CORE = (PREC == GEXS_FP32 && PK == PK_VOIGT);
+    static constexpr size_t raw_d = (size_t)2 * NT * sizeof(double);   /* one f64 array, 2 bufs */
+    static constexpr size_t off_nu = 0;
+    static constexpr size_t off_el = off_nu + raw_d;
+    static constexpr size_t off_ai = off_el + raw_d;
+    static constexpr size_t off_ga = off_ai + raw_d;
+    static constexpr size_t off_ne = off_ga + (PRESS ? raw_d : 0);
+    static constexpr size_t off_gn = off_ne + (PRESS ? raw_d : 0);
+    static constexpr size_t off_rec = (off_gn + (size_t)2 * NT * sizeof(int) + 15) & ~size_t(15);
+    static constexpr size_t rec_sz = (PREC == GEXS_FP32) ? sizeof(RecF32) : sizeof(RecF64);
+    static constexpr size_t off_core = off_rec + (size_t)R * rec_sz;
+    static constexpr size_t off_wacc = (off_core + (CORE ? (size_t)R * sizeof(CoreF64) : 0) + 15) & ~size_t(15);
+    static constexpr size_t bytes = off_wacc + (CORE ? (size_t)WARPS * W * sizeof(float) : 0);
+};
+
+/* ---------------------------------------------------------------- kernel */
+/* resident CTAs per SM the register budget is sized for */
+template <int B, int WARPS>
+constexpr int min_ctas() { return WARPS == 8 ? (B == 8 ? 2 : 3) : (B == 8 ? 4 : 6); }
+
+template <int PK, int PREC, int B, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, min_ctas<B, WARPS>())
 tile_kernel(const KArgs args)
 {
-    constexpr int NT = WARPS * 32;
+    typedef Smem<PK, PREC, B, WARPS> L;
+    constexpr int NT = L::NT;
+    constexpr int R = L::R;
     constexpr int W = 32 * B * WARPS;
-    constexpr bool PRESS = (PK != PK_ERF);
     typedef typename RecOf<PREC>::T Rec;
 
-    __shared__ double s_nu[2][NT];
-    __shared__ double s_el[2][NT];
-    __shared__ double s_ai[2][NT];
-    __shared__ double s_ga[2][PRESS ? NT : 1];
-    __shared__ double s_ne[2][PRESS ? NT : 1];
-    __shared__ int    s_gn[2][NT];
-    __shared__ Rec    s_rec[NT];
-    __shared__ int    s_item;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* s_nu = reinterpret_cast<double*>(smem + L::off_nu);
+    double* s_el = reinterpret_cast<double*>(smem + L::off_el);
+    double* s_ai = reinterpret_cast<double*>(smem + L::off_ai);
+    double* s_ga = reinterpret_cast<double*>(smem + L::off_ga);
+    double* s_ne = reinterpret_cast<double*>(smem + L::off_ne);
+    int*    s_gn = reinterpret_cast<int*>(smem + L::off_gn);
+    Rec*    s_rec = reinterpret_cast<Rec*>(smem + L::off_rec);
+    CoreF64* s_core = reinterpret_cast<CoreF64*>(smem + L::off_core);
+    float*  s_wacc = reinterpret_cast<float*>(smem + L::off_wacc);
+    __shared__ int s_item;
     __shared__ long long s_lohi[2];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wb = warp * 32 * B;          /* warp's first bin (tile-relative) */
     const double zthr = (PREC == GEXS_FP32) ? 10.5 : 27.5;
 
     for (;;) {
@@ -486,29 +639,35 @@ tile_kernel(const KArgs args)
         __syncthreads();
         const int64_t lo = s_lohi[0];
         const int64_t hi = max((int64_t)s_lohi[1], lo);
-        const int nst = (int)((hi - lo + NT - 1) / NT);
+        const int nph = (int)((hi - lo + R - 1) / R);
+        if constexpr (L::CORE) {
+            for (int z = tid; z < WARPS * W; z += NT) s_wacc[z] = 0.f;
+            __syncthreads();
+        }
 
-        /* per-lane accumulators */
-        float  ks[B], kc[B], part[B], lk[B];
+        float  ks[B], kc[B], part[B];
         double acc[B], fbin[B];
 #pragma unroll
         for (int k = 0; k < B; ++k) {
             ks[k] = kc[k] = part[k] = 0.f; acc[k] = 0.0;
-            lk[k] = (float)(lane + 32 * k);
-            fbin[k] = grid_f(J.nu_start, J.dnu, T.j0 + wb + lane + 32 * k);
+            if (PREC == GEXS_FP64) fbin[k] = grid_f(J.nu_start, J.dnu, T.j0 + warp * 32 * B + lane + 32 * k);
         }
 
-        auto issue = [&](int s) {
-            int64_t i = lo + (int64_t)s * NT + tid;
-            int buf = s & 1;
-            if (s < nst && i < hi) {
-                cp_async8(&s_nu[buf][tid], J.lines.nu + i);
-                cp_async8(&s_el[buf][tid], J.lines.elow + i);
-                cp_async8(&s_ai[buf][tid], J.lines.aif + i);
-                cp_async4(&s_gn[buf][tid], J.lines.gns + i);
-                if constexpr (PRESS) {
-                    cp_async8(&s_ga[buf][tid], J.lines.gamma + i);
-                    cp_async8(&s_ne[buf][tid], J.lines.n + i);
+        /* thread tid stages and derives lines lo + u*NT + tid, u = 0, 1, ...;
+         * every thread only ever reads the staging slots it filled itself,
+         * so the double-buffered cp.async pipeline needs no barrier */
+        const int nsub = nph * PH;
+        auto issue = [&](int u) {
+            const int64_t i = lo + (int64_t)u * NT + tid;
+            const int o = (u & 1) * NT + tid;
+            if (u < nsub && i < hi) {
+                cp_async8(s_nu + o, J.lines.nu + i);
+                cp_async8(s_el + o, J.lines.elow + i);
+                cp_async8(s_ai + o, J.lines.aif + i);
+                cp_async4(s_gn + o, J.lines.gns + i);
+                if constexpr (L::PRESS) {
+                    cp_async8(s_ga + o, J.lines.gamma + i);
+                    cp_async8(s_ne + o, J.lines.n + i);
                 }
             }
             cp_async_commit();
@@ -516,31 +675,51 @@ tile_kernel(const KArgs args)
         issue(0);
         issue(1);
 
-        for (int s = 0; s < nst; ++s) {
-            const int buf = s & 1;
-            cp_async_wait<1>();
-            __syncthreads();
-            const int nrec = (int)min((int64_t)NT, hi - lo - (int64_t)s * NT);
-            if (tid < nrec) {
-                RawLine L;
-                L.nu = s_nu[buf][tid]; L.elow = s_el[buf][tid]; L.aif = s_ai[buf][tid];
-                L.g = s_gn[buf][tid];
-                if constexpr (PRESS) { L.gam = s_ga[buf][tid]; L.nexp = s_ne[buf][tid]; }
-                else { L.gam = 0.0; L.nexp = 0.0; }
-                Derived<PK> d = derive_line<PK>(T, L, zthr);
-                Rec r;
-                make_rec<PK>(r, d, J, T);
-                s_rec[tid] = r;
+        for (int ph = 0; ph < nph; ++ph) {
+            const int64_t pbase = lo + (int64_t)ph * R;
+            const int nrec = (int)min((int64_t)R, hi - pbase);
+#pragma unroll
+            for (int sub = 0; sub < PH; ++sub) {
+                const int u = ph * PH + sub;
+                const int o = (u & 1) * NT + tid;
+                cp_async_wait<1>();
+                const int r = sub * NT + tid;
+                if (r < nrec) {
+                    RawLine Lr;
+                    Lr.nu = s_nu[o]; Lr.elow = s_el[o]; Lr.aif = s_ai[o]; Lr.g = s_gn[o];
+                    if constexpr (L::PRESS) { Lr.gam = s_ga[o]; Lr.nexp = s_ne[o]; }
+                    else { Lr.gam = 0.0; Lr.nexp = 0.0; }
+                    Derived<PK> d = derive_line<PK>(T, Lr, zthr);
+                    Rec rr;
+                    make_rec<PK, B, WARPS>(rr, d, J, T);
+                    s_rec[r] = rr;
+                    if constexpr (L::CORE) {
+                        CoreF64 cd;
+                        cd.nu = d.nu; cd.invw = d.invw; cd.y = d.y;
+                        cd.amp = dmul(dmul(d.S, d.invw), J.out_scale);
+                        cd.c2 = d.c2; cd.c3 = d.c3;
+                        s_core[r] = cd;
+                    }
+                }
+                issue(u + 2);
             }
             __syncthreads();
-            issue(s + 2);
 
             if constexpr (PREC == GEXS_FP32) {
-                lines_f32<PK, B>(s_rec, nrec, wb, lane, lk, part);
+                /* Kahan merge of FP32 partial sums every 128 lines */
+                for (int c0 = 0; c0 < nrec; c0 += 128) {
+                    const int cn = min(128, nrec - c0);
+                    lines_f32<PK, B>(reinterpret_cast<const RecF32*>(s_rec) + c0, s_core + c0, cn,
+                                     warp, lane, part, J.nu_start, J.dnu, T.j0);
 #pragma unroll
-                for (int k = 0; k < B; ++k) { kahan_add(ks[k], kc[k], part[k]); part[k] = 0.f; }
+                    for (int k = 0; k < B; ++k) { kahan_add(ks[k], kc[k], part[k]); part[k] = 0.f; }
+                }
+                if constexpr (L::CORE)
+                    core_pass_f32<WARPS>(reinterpret_cast<const RecF32*>(s_rec), s_core, nrec, warp,
+                                         lane, s_wacc + warp * W, J.nu_start, J.dnu, T.j0);
             } else {
-                lines_f64<PK, B>(s_rec, nrec, wb, lane, fbin, acc, J);
+                lines_f64<PK, B>(reinterpret_cast<const RecF64*>(s_rec), nrec, warp, lane, fbin,
+                                 acc, J);
             }
             __syncthreads();
         }
@@ -551,9 +730,14 @@ tile_kernel(const KArgs args)
         const int acc_mode = J.accumulate;
 #pragma unroll
         for (int k = 0; k < B; ++k) {
-            const int t = wb + lane + 32 * k;
+            const int t = warp * 32 * B + lane + 32 * k;
             if (t < T.jn) {
                 double v = (PREC == GEXS_FP32) ? ((double)ks[k] - (double)kc[k]) : acc[k];
+                if constexpr (L::CORE) {
+                    /* core terms of every warp row, in warp order */
+#pragma unroll
+                    for (int w2 = 0; w2 < WARPS; ++w2) v += (double)s_wacc[w2 * W + t];
+                }
                 int64_t j = T.j0 + t;
                 out[j] = acc_mode ? out[j] + v : v;
             }
@@ -630,14 +814,17 @@ template <int PK, int PREC, int B, int WARPS>
 static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st)
 {
     auto kern = tile_kernel<PK, PREC, B, WARPS>;
+    const size_t smem = Smem<PK, PREC, B, WARPS>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, WARPS * 32, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     int per = ctas_per_sm > 0 ? min(ctas_per_sm, occ) : occ;
     int grid = min(a.nitems, per * nsm);
     if (grid < 1) grid = 1;
-    kern<<<grid, WARPS * 32, 0, st>>>(a);
+    kern<<<grid, WARPS * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 

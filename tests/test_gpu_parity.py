@@ -195,3 +195,15 @@ def test_eval_count_matches_oracle(gpu_ctx, small_lines):
     got = gpu_ctx.count_evals(jobs)
     want = [po.count_evals(H.host_job(j.c, small_lines)) for j in jobs]
     assert got == want
+
+
+@pytest.mark.parametrize("T,P,dnu", [(100.0, 1e-5, 0.1), (300.0, 1e-3, 0.1), (100.0, 1e-5, 0.005),
+                                     (3000.0, 100.0, 0.1)])
+def test_fp32_narrow_and_broad_lines(gpu_ctx, small_lines, T, P, dnu):
+    """Lines far narrower than a bin (the nearest bins sit in the steep
+    Doppler core) and pressure-broadened lines wider than many bins."""
+    G = int(round(3900.0 / dnu)) + 1
+    for prof in (capi.VOIGT, capi.DOPPLER):
+        job = _make(small_lines, capi.FP32, prof, 16, capi.CONV_PHYSICAL, T=T, P=P, dnu=dnu, G=G,
+                    cutoff=25.0)
+        _check(gpu_ctx, job, small_lines)
