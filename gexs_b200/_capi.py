@@ -10,7 +10,10 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgexs_b200.so")
 
 GEXS_OK = 0
+GEXS_ERR_INVALID = -1
+GEXS_ERR_TIMEOUT = -4
 GEXS_ERR_NOT_READY = -5
+GEXS_ERR_ADMISSION = -6
 NOALLOC_MAX_JOBS = 64
 
 GAUSSIAN, DOPPLER, VOIGT, VOIGT_QUAD = 0, 1, 2, 4
@@ -44,7 +47,23 @@ class GexsLaunchCfg(C.Structure):
                 ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32)]
 
 
-# (name, restype, argtypes) for every symbol of include/gexs_b200.h
+class GexsRequest(C.Structure):
+    _fields_ = [("list_id", C.c_int32), ("profile", C.c_int32), ("precision", C.c_int32),
+                ("convention", C.c_int32), ("quad_nodes", C.c_int32), ("reserved", C.c_int32),
+                ("temperature", C.c_double), ("pressure", C.c_double),
+                ("nu_start", C.c_double), ("dnu", C.c_double), ("grid_points", C.c_int64),
+                ("cutoff", C.c_double), ("half_width", C.c_double), ("ref_temp", C.c_double),
+                ("ref_press", C.c_double)]
+
+
+class GexsRequestInfo(C.Structure):
+    _fields_ = [("submit_ms", C.c_double), ("admit_ms", C.c_double), ("done_ms", C.c_double),
+                ("fetched_ms", C.c_double), ("evals", C.c_int64), ("batch_size", C.c_int32),
+                ("status", C.c_int32)]
+
+
+# (name, restype, argtypes) for every symbol of include/gexs_b200.h and
+# include/gexs_serve.h
 SIGNATURES = [
     ("gexs_version", C.c_int, []),
     ("gexs_status_string", C.c_char_p, [C.c_int]),
@@ -85,6 +104,16 @@ SIGNATURES = [
                                                 C.c_int, C.c_int]),
     ("gexs_manager_ntrans", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("gexs_manager_ready", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("gexs_server_create", C.c_int, [C.c_int, C.c_size_t, C.c_int, C.c_int,
+                                     C.POINTER(C.c_void_p)]),
+    ("gexs_server_destroy", C.c_int, [C.c_void_p]),
+    ("gexs_server_add_list", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 +
+     [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int)]),
+    ("gexs_server_submit", C.c_int, [C.c_void_p, C.POINTER(GexsRequest), C.POINTER(C.c_uint64)]),
+    ("gexs_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p,
+                                   C.POINTER(GexsRequestInfo)]),
+    ("gexs_server_poll", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("gexs_server_stats", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 4),
 ]
 
 _lib = None

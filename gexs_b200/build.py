@@ -23,6 +23,7 @@ SOURCES = [
     "csrc/gexs_calib.cu",
     "csrc/gexs_noalloc.cu",
     "host/B200Manager.cpp",
+    "host/gexs_server.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")
 
@@ -43,6 +44,7 @@ def build(ptxas_verbose=False, force=False):
     for root, _, files in os.walk(os.path.join(HERE, "host")):
         deps += [os.path.join(root, f) for f in files]
     deps.append(os.path.join(ROOT, "include", "gexs_b200.h"))
+    deps.append(os.path.join(ROOT, "include", "gexs_serve.h"))
     newest = max(os.path.getmtime(d) for d in deps)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB

@@ -251,3 +251,78 @@ class Manager:
         v = C.c_int()
         check(lib().gexs_manager_ready(self.h, C.byref(v)), "ReadyForWork")
         return bool(v.value)
+
+
+class Server:
+    """Continuous-batching request loop (include/gexs_serve.h)."""
+
+    def __init__(self, device=0, hbm_budget=0, max_inflight=0, streams=0):
+        self.h = C.c_void_p()
+        check(lib().gexs_server_create(device, int(hbm_budget), max_inflight, streams,
+                                       C.byref(self.h)), "gexs_server_create")
+
+    def close(self):
+        if self.h:
+            lib().gexs_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _p(a):
+        return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+    def add_list(self, lines, state_energy, state_g, mass):
+        """lines: dict of host numpy arrays (nu, elow, aif, gns[, gamma, n])."""
+        lid = C.c_int()
+        se = np.ascontiguousarray(state_energy, dtype=np.float64)
+        sg = np.ascontiguousarray(state_g, dtype=np.int32)
+        check(lib().gexs_server_add_list(
+            self.h, self._p(lines["nu"]), self._p(lines["elow"]), self._p(lines["aif"]),
+            self._p(lines["gns"]), self._p(lines.get("gamma")), self._p(lines.get("n")),
+            len(lines["nu"]), self._p(se), self._p(sg), len(se), float(mass), C.byref(lid)),
+            "gexs_server_add_list")
+        return lid.value
+
+    @staticmethod
+    def request(list_id, profile, temperature, pressure, nu_start, dnu, grid_points,
+                precision=capi.FP32, convention=capi.CONV_PHYSICAL, cutoff=-1.0, quad_nodes=16,
+                half_width=0.0, ref_temp=296.0, ref_press=1.0):
+        return capi.GexsRequest(list_id, profile, precision, convention, quad_nodes, 0,
+                                temperature, pressure, nu_start, dnu, int(grid_points), cutoff,
+                                half_width, ref_temp, ref_press)
+
+    def submit(self, req):
+        t = C.c_uint64()
+        st = lib().gexs_server_submit(self.h, C.byref(req), C.byref(t))
+        check(st, "gexs_server_submit")
+        return t.value
+
+    def try_submit(self, req):
+        t = C.c_uint64()
+        st = lib().gexs_server_submit(self.h, C.byref(req), C.byref(t))
+        return st, t.value
+
+    def wait(self, ticket, grid_points, timeout_ms=-1):
+        out = np.empty(int(grid_points), dtype=np.float64)
+        info = capi.GexsRequestInfo()
+        check(lib().gexs_server_wait(self.h, ticket, timeout_ms, self._p(out), C.byref(info)),
+              "gexs_server_wait")
+        return out, info
+
+    def wait_status(self, ticket, timeout_ms):
+        info = capi.GexsRequestInfo()
+        return lib().gexs_server_wait(self.h, ticket, timeout_ms, None, C.byref(info))
+
+    def poll(self, ticket):
+        return lib().gexs_server_poll(self.h, ticket)
+
+    def stats(self):
+        v = [C.c_int64() for _ in range(4)]
+        check(lib().gexs_server_stats(self.h, *[C.byref(x) for x in v]), "gexs_server_stats")
+        return {"submitted": v[0].value, "completed": v[1].value, "batches": v[2].value,
+                "inflight_bytes": v[3].value}

@@ -1,0 +1,515 @@
+/*
+ * gexs_server.cpp — continuous-batching request loop (include/gexs_serve.h).
+ *
+ * One worker thread owns admission and launches:
+ *   1. completed batches are detected with cudaEventQuery and their
+ *      requests marked done (waiters are woken);
+ *   2. pending requests are admitted in arrival order while their output
+ *      grids fit in the HBM budget and the in-flight cap allows;
+ *   3. the admitted group gets Q(T) from the resident states (partition
+ *      kernel on the worker's own stream), stream-ordered output buffers
+ *      (cudaMallocAsync) and one gexs_run launch on the next stream of the
+ *      pool, followed by an event.
+ * Nothing on this path synchronises the device (no cudaMalloc/cudaFree),
+ * so a new batch starts while earlier ones still run.  A request's output
+ * is released when the caller fetches it (gexs_server_wait), which frees
+ * budget for the next admissions.
+ */
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+#include "../../include/gexs_serve.h"
+#include "../csrc/gexs_internal.h"
+
+namespace {
+
+enum { RQ_PENDING = 0, RQ_RUNNING = 1, RQ_DONE = 2, RQ_FAILED = 3 };
+
+struct List {
+    double *nu = nullptr, *elow = nullptr, *aif = nullptr, *gamma = nullptr, *n = nullptr;
+    int32_t* gns = nullptr;
+    int64_t count = 0;
+    double* se = nullptr;
+    int32_t* sg = nullptr;
+    int64_t nstates = 0;
+    double mass = 0.0;
+    size_t bytes = 0;
+};
+
+struct Req {
+    uint64_t id = 0;
+    gexs_request r;
+    gexs_job job;
+    double* d_out = nullptr;
+    size_t bytes = 0;
+    int state = RQ_PENDING;
+    int status = GEXS_OK;
+    cudaEvent_t done = nullptr;        /* owned by the batch */
+    gexs_request_info info;
+};
+
+struct Batch {
+    cudaEvent_t ev = nullptr;
+    std::vector<Req*> reqs;
+};
+
+constexpr int kMaxBatchTemps = 1024;
+
+}  // namespace
+
+struct gexs_server {
+    int device = 0;
+    size_t budget = 0;
+    int max_inflight = 256;
+    gexs_ctx* ctx = nullptr;
+    std::vector<cudaStream_t> streams;
+    size_t next_stream = 0;
+    cudaStream_t part_stream = nullptr;
+    double *d_betas = nullptr, *d_partial = nullptr, *d_q = nullptr;
+    int part_chunks = 0;
+    int nsm = 148;
+
+    std::vector<List> lists;
+    size_t resident = 0;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req*> pending;
+    std::unordered_map<uint64_t, Req*> reqs;
+    std::vector<Batch> running;
+    size_t inflight_bytes = 0;
+    int inflight = 0;
+    uint64_t next_id = 1;
+    bool stop = false;
+    bool kick = false;            /* a submission or a released output */
+    std::thread worker;
+
+    std::mutex copy_mu;
+    std::vector<cudaStream_t> copy_free;
+
+    int64_t n_submitted = 0, n_completed = 0, n_batches = 0;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+    double now_ms() const
+    {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+size_t output_bytes(const gexs_request& r) { return (size_t)r.grid_points * sizeof(double); }
+
+/* Q(T) for the admitted requests of one list: the partition kernel on the
+ * server's own stream (no device-wide synchronisation). */
+int partitions(gexs_server* s, const List& L, const std::vector<double>& temps, std::vector<double>& q)
+{
+    const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+    q.assign(temps.size(), 0.0);
+    for (size_t off = 0; off < temps.size(); off += kMaxBatchTemps) {
+        int nt = (int)std::min<size_t>(kMaxBatchTemps, temps.size() - off);
+        std::vector<double> betas(nt);
+        for (int i = 0; i < nt; ++i) betas[i] = planck * vellgt / (boltz * temps[off + i]);
+        cudaError_t e = cudaMemcpyAsync(s->d_betas, betas.data(), sizeof(double) * nt,
+                                        cudaMemcpyHostToDevice, s->part_stream);
+        if (e == cudaSuccess)
+            e = gexs::launch_partition(L.se, L.sg, L.nstates, s->d_betas, nt, s->d_partial,
+                                       s->part_chunks, s->d_q, s->part_stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(q.data() + off, s->d_q, sizeof(double) * nt,
+                                cudaMemcpyDeviceToHost, s->part_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->part_stream);
+        if (e != cudaSuccess) return gexs::cuda_error(e, "server partition");
+    }
+    return GEXS_OK;
+}
+
+/* build jobs, allocate outputs and launch one group; called without the lock */
+void launch_group(gexs_server* s, std::vector<Req*>& adm)
+{
+    cudaSetDevice(s->device);
+    cudaStream_t st = s->streams[s->next_stream++ % s->streams.size()];
+    int status = GEXS_OK;
+    std::map<int, std::vector<Req*>> by_list;
+    for (Req* r : adm) by_list[r->r.list_id].push_back(r);
+    std::vector<gexs_job> jobs;
+    for (auto& kv : by_list) {
+        const List& L = s->lists[kv.first];
+        std::vector<double> temps, q;
+        for (Req* r : kv.second) temps.push_back(r->r.temperature);
+        if (!status) status = partitions(s, L, temps, q);
+        for (size_t i = 0; i < kv.second.size() && !status; ++i) {
+            Req* r = kv.second[i];
+            gexs_job j;
+            status = gexs_job_init(&j, r->r.convention, r->r.profile, r->r.temperature,
+                                   r->r.pressure, q[i], L.mass, r->r.ref_temp, r->r.ref_press,
+                                   r->r.half_width, r->r.cutoff, r->r.nu_start, r->r.dnu,
+                                   r->r.grid_points);
+            if (status) break;
+            j.precision = r->r.precision;
+            j.quad_nodes = r->r.quad_nodes;
+            j.accumulate = 0;
+            j.lines.nu = L.nu; j.lines.elow = L.elow; j.lines.aif = L.aif; j.lines.gns = L.gns;
+            j.lines.gamma = L.gamma; j.lines.n = L.n; j.lines.count = L.count;
+            void* d = nullptr;
+            if (cudaMallocAsync(&d, r->bytes, st) != cudaSuccess) { status = GEXS_ERR_OOM; break; }
+            r->d_out = (double*)d;
+            j.out = r->d_out;
+            r->job = j;
+            jobs.push_back(j);
+        }
+    }
+    Batch b;
+    if (!status) status = gexs_run(s->ctx, jobs.data(), (int)jobs.size(), nullptr, (void*)st);
+    if (!status && cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming) != cudaSuccess)
+        status = GEXS_ERR_CUDA;
+    if (!status && cudaEventRecord(b.ev, st) != cudaSuccess) status = GEXS_ERR_CUDA;
+    std::lock_guard<std::mutex> g(s->mu);
+    s->n_batches++;
+    for (Req* r : adm) {
+        r->info.batch_size = (int)adm.size();
+        if (status) {
+            r->state = RQ_FAILED;
+            r->status = status;
+            r->info.done_ms = s->now_ms();
+        } else {
+            r->state = RQ_RUNNING;
+            r->done = b.ev;
+        }
+    }
+    if (status) {
+        if (b.ev) cudaEventDestroy(b.ev);
+        for (Req* r : adm)
+            if (r->d_out) { cudaFreeAsync(r->d_out, st); r->d_out = nullptr; }
+        s->cv_done.notify_all();
+        return;
+    }
+    b.reqs = adm;
+    s->running.push_back(b);
+}
+
+void worker_loop(gexs_server* s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        /* sleep until kicked, or poll running batches every 100 us */
+        s->cv_work.wait_for(lk, std::chrono::microseconds(s->running.empty() ? 20000 : 100),
+                            [&] { return s->stop || s->kick; });
+        s->kick = false;
+        /* 1. completions */
+        for (size_t i = 0; i < s->running.size();) {
+            cudaError_t q = cudaEventQuery(s->running[i].ev);
+            if (q == cudaErrorNotReady) { ++i; continue; }
+            double t = s->now_ms();
+            for (Req* r : s->running[i].reqs) {
+                r->state = (q == cudaSuccess) ? RQ_DONE : RQ_FAILED;
+                if (q != cudaSuccess) r->status = GEXS_ERR_CUDA;
+                r->info.done_ms = t;
+                r->info.status = r->status;
+                s->n_completed++;
+            }
+            /* the event is destroyed when its last request is fetched */
+            s->running.erase(s->running.begin() + i);
+            s->cv_done.notify_all();
+        }
+        if (s->stop && s->running.empty()) break;
+        if (s->stop) continue;
+        /* 2. admission in arrival order */
+        const size_t cap = s->budget > s->resident ? s->budget - s->resident : 0;
+        std::vector<Req*> adm;
+        while (!s->pending.empty()) {
+            Req* r = s->pending.front();
+            if (s->inflight >= s->max_inflight || s->inflight_bytes + r->bytes > cap) break;
+            s->pending.pop_front();
+            s->inflight++;
+            s->inflight_bytes += r->bytes;
+            r->info.admit_ms = s->now_ms();
+            adm.push_back(r);
+        }
+        if (!adm.empty()) {
+            lk.unlock();
+            launch_group(s, adm);
+            lk.lock();
+        }
+    }
+    /* requests never admitted */
+    for (Req* r : s->pending) { r->state = RQ_FAILED; r->status = GEXS_ERR_SHUTDOWN; }
+    s->pending.clear();
+    s->cv_done.notify_all();
+}
+
+cudaStream_t take_copy_stream(gexs_server* s)
+{
+    std::lock_guard<std::mutex> g(s->copy_mu);
+    if (!s->copy_free.empty()) {
+        cudaStream_t c = s->copy_free.back();
+        s->copy_free.pop_back();
+        return c;
+    }
+    cudaStream_t c = nullptr;
+    cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking);
+    return c;
+}
+
+void give_copy_stream(gexs_server* s, cudaStream_t c)
+{
+    std::lock_guard<std::mutex> g(s->copy_mu);
+    s->copy_free.push_back(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int streams,
+                       gexs_server** out)
+{
+    if (!out) return gexs::set_error(GEXS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return gexs::cuda_error(e, "cudaSetDevice");
+    gexs_server* s = new gexs_server();
+    s->device = device;
+    int st = gexs_ctx_create(device, &s->ctx);
+    if (st) { delete s; return st; }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    s->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+    s->max_inflight = max_inflight > 0 ? max_inflight : 256;
+    int ns = streams > 0 ? streams : 4;
+    for (int i = 0; i < ns; ++i) {
+        cudaStream_t c;
+        cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking);
+        s->streams.push_back(c);
+    }
+    cudaStreamCreateWithFlags(&s->part_stream, cudaStreamNonBlocking);
+    cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, device);
+    s->part_chunks = s->nsm * 2;
+    bool ok = cudaMalloc(&s->d_betas, sizeof(double) * kMaxBatchTemps) == cudaSuccess &&
+              cudaMalloc(&s->d_partial, sizeof(double) * kMaxBatchTemps * s->part_chunks) == cudaSuccess &&
+              cudaMalloc(&s->d_q, sizeof(double) * kMaxBatchTemps) == cudaSuccess;
+    if (!ok) { gexs_server_destroy(s); return gexs::set_error(GEXS_ERR_OOM, "server buffers"); }
+    s->worker = std::thread(worker_loop, s);
+    *out = s;
+    return GEXS_OK;
+}
+
+int gexs_server_destroy(gexs_server* s)
+{
+    if (!s) return GEXS_OK;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->device);
+    cudaDeviceSynchronize();
+    for (auto& kv : s->reqs) {
+        Req* r = kv.second;
+        if (r->d_out) cudaFree(r->d_out);
+        delete r;
+    }
+    for (Batch& b : s->running) cudaEventDestroy(b.ev);
+    for (List& L : s->lists) {
+        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
+        cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.se); cudaFree(L.sg);
+    }
+    for (cudaStream_t c : s->streams) cudaStreamDestroy(c);
+    for (cudaStream_t c : s->copy_free) cudaStreamDestroy(c);
+    if (s->part_stream) cudaStreamDestroy(s->part_stream);
+    cudaFree(s->d_betas); cudaFree(s->d_partial); cudaFree(s->d_q);
+    gexs_ctx_destroy(s->ctx);
+    delete s;
+    return GEXS_OK;
+}
+
+int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow, const double* aif,
+                         const int32_t* gns, const double* gamma, const double* n, int64_t count,
+                         const double* state_energy, const int32_t* state_g, int64_t nstates,
+                         double mean_mass, int* list_id)
+{
+    if (!s || !list_id || count < 0 || nstates <= 0 || !state_energy || !state_g ||
+        (count > 0 && (!nu || !elow || !aif || !gns)) || !(mean_mass > 0.0))
+        return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_add_list: arguments");
+    const bool press = gamma && n;
+    size_t bytes = (size_t)count * (3 * sizeof(double) + sizeof(int32_t) + (press ? 2 * sizeof(double) : 0)) +
+                   (size_t)nstates * (sizeof(double) + sizeof(int32_t));
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (s->resident + s->inflight_bytes + bytes > s->budget)
+            return gexs::set_error(GEXS_ERR_ADMISSION, "line list does not fit in the HBM budget");
+    }
+    cudaSetDevice(s->device);
+    List L;
+    L.count = count; L.nstates = nstates; L.mass = mean_mass; L.bytes = bytes;
+    size_t c = (size_t)(count > 0 ? count : 1);
+    bool ok = cudaMalloc(&L.nu, sizeof(double) * c) == cudaSuccess &&
+              cudaMalloc(&L.elow, sizeof(double) * c) == cudaSuccess &&
+              cudaMalloc(&L.aif, sizeof(double) * c) == cudaSuccess &&
+              cudaMalloc(&L.gns, sizeof(int32_t) * c) == cudaSuccess &&
+              cudaMalloc(&L.se, sizeof(double) * nstates) == cudaSuccess &&
+              cudaMalloc(&L.sg, sizeof(int32_t) * nstates) == cudaSuccess;
+    if (ok && press)
+        ok = cudaMalloc(&L.gamma, sizeof(double) * c) == cudaSuccess &&
+             cudaMalloc(&L.n, sizeof(double) * c) == cudaSuccess;
+    if (!ok) {
+        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
+        cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n);
+        return gexs::set_error(GEXS_ERR_OOM, "line list upload");
+    }
+    if (count > 0) {
+        cudaMemcpy(L.nu, nu, sizeof(double) * count, cudaMemcpyDefault);
+        cudaMemcpy(L.elow, elow, sizeof(double) * count, cudaMemcpyDefault);
+        cudaMemcpy(L.aif, aif, sizeof(double) * count, cudaMemcpyDefault);
+        cudaMemcpy(L.gns, gns, sizeof(int32_t) * count, cudaMemcpyDefault);
+        if (press) {
+            cudaMemcpy(L.gamma, gamma, sizeof(double) * count, cudaMemcpyDefault);
+            cudaMemcpy(L.n, n, sizeof(double) * count, cudaMemcpyDefault);
+        }
+    }
+    cudaMemcpy(L.se, state_energy, sizeof(double) * nstates, cudaMemcpyDefault);
+    cudaError_t e = cudaMemcpy(L.sg, state_g, sizeof(int32_t) * nstates, cudaMemcpyDefault);
+    if (e != cudaSuccess) return gexs::cuda_error(e, "line list upload");
+    std::lock_guard<std::mutex> g(s->mu);
+    s->lists.push_back(L);
+    s->resident += bytes;
+    *list_id = (int)s->lists.size() - 1;
+    return GEXS_OK;
+}
+
+int gexs_server_submit(gexs_server* s, const gexs_request* r, uint64_t* ticket)
+{
+    if (!s || !r || !ticket) return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_submit: arguments");
+    gexs_job probe;
+    int st = gexs_job_init(&probe, r->convention, r->profile, r->temperature, r->pressure, 1.0, 1.0,
+                           r->ref_temp > 0 ? r->ref_temp : 296.0, r->ref_press, r->half_width,
+                           r->cutoff, r->nu_start, r->dnu, r->grid_points);
+    if (st) return st;
+    if (r->precision != GEXS_FP32 && r->precision != GEXS_FP64)
+        return gexs::set_error(GEXS_ERR_INVALID, "precision");
+    if (r->profile == GEXS_VOIGT_QUAD && r->quad_nodes != 16 && r->quad_nodes != 32)
+        return gexs::set_error(GEXS_ERR_INVALID, "quad_nodes");
+    Req* q = new Req();
+    q->r = *r;
+    if (!(q->r.ref_temp > 0)) q->r.ref_temp = 296.0;
+    if (q->r.profile != GEXS_VOIGT_QUAD) q->r.quad_nodes = 16;
+    q->bytes = output_bytes(*r);
+    std::memset(&q->info, 0, sizeof(q->info));
+    q->info.evals = -1;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (r->list_id < 0 || r->list_id >= (int)s->lists.size()) {
+            delete q;
+            return gexs::set_error(GEXS_ERR_INVALID, "unknown list_id");
+        }
+        const List& L = s->lists[r->list_id];
+        bool press = r->profile == GEXS_VOIGT || r->profile == GEXS_VOIGT_QUAD;
+        if (press && !L.gamma) {
+            delete q;
+            return gexs::set_error(GEXS_ERR_INVALID, "list has no broadening for this profile");
+        }
+        if (s->resident + q->bytes > s->budget) {
+            delete q;
+            return gexs::set_error(GEXS_ERR_ADMISSION, "request output exceeds the HBM budget");
+        }
+        if (s->stop) { delete q; return gexs::set_error(GEXS_ERR_SHUTDOWN, "server stopping"); }
+        q->id = s->next_id++;
+        q->info.submit_ms = s->now_ms();
+        s->reqs[q->id] = q;
+        s->pending.push_back(q);
+        s->n_submitted++;
+        s->kick = true;
+        *ticket = q->id;
+    }
+    s->cv_work.notify_one();
+    return GEXS_OK;
+}
+
+int gexs_server_poll(gexs_server* s, uint64_t ticket)
+{
+    if (!s) return GEXS_ERR_INVALID;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return gexs::set_error(GEXS_ERR_INVALID, "unknown ticket");
+    int state = it->second->state;
+    if (state == RQ_DONE) return GEXS_OK;
+    if (state == RQ_FAILED) return it->second->status;
+    return GEXS_ERR_NOT_READY;
+}
+
+int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_out,
+                     gexs_request_info* info)
+{
+    if (!s) return GEXS_ERR_INVALID;
+    Req* r = nullptr;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return gexs::set_error(GEXS_ERR_INVALID, "unknown ticket");
+        r = it->second;
+        auto ready = [&] { return r->state == RQ_DONE || r->state == RQ_FAILED; };
+        if (timeout_ms < 0) s->cv_done.wait(lk, ready);
+        else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+            return gexs::set_error(GEXS_ERR_TIMEOUT, "request not finished");
+        s->reqs.erase(it);
+    }
+    int status = r->state == RQ_DONE ? GEXS_OK : r->status;
+    cudaSetDevice(s->device);
+    if (r->d_out) {
+        cudaStream_t c = take_copy_stream(s);
+        cudaError_t e = cudaSuccess;
+        if (r->done) e = cudaStreamWaitEvent(c, r->done, 0);
+        if (e == cudaSuccess && h_out && !status)
+            e = cudaMemcpyAsync(h_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, c);
+        cudaError_t e2 = cudaFreeAsync(r->d_out, c);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c);
+        give_copy_stream(s, c);
+        if (e != cudaSuccess && !status) status = gexs::cuda_error(e, "result copy");
+        r->d_out = nullptr;
+    }
+    bool last_of_batch = true;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->inflight--;
+        s->inflight_bytes -= r->bytes;
+        r->info.fetched_ms = s->now_ms();
+        r->info.status = status;
+        s->kick = true;
+        if (r->done)
+            for (auto& kv : s->reqs)
+                if (kv.second->done == r->done) { last_of_batch = false; break; }
+    }
+    if (r->done && last_of_batch) cudaEventDestroy(r->done);
+    if (info) *info = r->info;
+    delete r;
+    s->cv_work.notify_one();
+    if (status) return gexs::set_error(status, "request failed");
+    return GEXS_OK;
+}
+
+int gexs_server_stats(gexs_server* s, int64_t* submitted, int64_t* completed, int64_t* batches,
+                      int64_t* inflight_bytes)
+{
+    if (!s) return GEXS_ERR_INVALID;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (submitted) *submitted = s->n_submitted;
+    if (completed) *completed = s->n_completed;
+    if (batches) *batches = s->n_batches;
+    if (inflight_bytes) *inflight_bytes = (int64_t)s->inflight_bytes;
+    return GEXS_OK;
+}
+
+}  // extern "C"

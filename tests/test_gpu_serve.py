@@ -1,0 +1,125 @@
+"""Request loop: admission by HBM budget, continuous batching, results
+identical alone and in a mix, failures reported per request."""
+import threading
+
+import numpy as np
+import pytest
+
+from gexs_b200 import _capi as capi
+from gexs_b200.engine import Server, job_init
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def served(small_states, small_lines):
+    srv = Server(0, hbm_budget=1 << 30, streams=4)
+    lid = srv.add_list(small_lines, small_states.energy, small_states.g, 18.0)
+    dop = {k: v for k, v in small_lines.items() if k not in ("gamma", "n")}
+    lid_dop = srv.add_list(dop, small_states.energy, small_states.g, 28.0)
+    yield srv, lid, lid_dop
+    srv.close()
+
+
+def _requests(lid, lid_dop, n=10, seed=5):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(n):
+        T = float(10 ** rng.uniform(2.0, np.log10(3000.0)))
+        P = float(10 ** rng.uniform(-6.0, 2.0))
+        d = float(10 ** rng.uniform(-2.5, -1.0))
+        nu0 = float(rng.uniform(100.0, 3000.0))
+        G = int(rng.integers(2000, 60000))
+        voigt = i % 2 == 0
+        out.append(Server.request(lid if voigt else lid_dop,
+                                  capi.VOIGT if voigt else capi.DOPPLER, T, P, nu0, d, G,
+                                  precision=capi.FP32 if i % 3 else capi.FP64, cutoff=25.0))
+    return out
+
+
+def test_alone_equals_mixed(served):
+    srv, lid, lid_dop = served
+    reqs = _requests(lid, lid_dop)
+    alone = []
+    for r in reqs:
+        t = srv.submit(r)
+        alone.append(srv.wait(t, r.grid_points)[0])
+    tickets = [srv.submit(r) for r in reqs]
+    mixed, sizes = [], []
+    for r, t in zip(reqs, tickets):
+        out, info = srv.wait(t, r.grid_points)
+        mixed.append(out)
+        sizes.append(info.batch_size)
+    for a, b in zip(alone, mixed):
+        np.testing.assert_array_equal(a, b)
+    assert max(sizes) > 1, "requests submitted together were never batched"
+
+
+def test_served_results_match_oracle(served, small_states, small_lines):
+    from oracle import pyoracle as po
+    srv, lid, lid_dop = served
+    for prof, prec, L, l_id, mass in ((capi.VOIGT, capi.FP64, small_lines, lid, 18.0),
+                                      (capi.DOPPLER, capi.FP64, small_lines, lid_dop, 28.0),
+                                      (capi.VOIGT, capi.FP32, small_lines, lid, 18.0)):
+        T, P, nu0, d, G = 900.0, 0.3, 500.0, 0.02, 50000
+        r = Server.request(l_id, prof, T, P, nu0, d, G, precision=prec, cutoff=25.0)
+        out, info = srv.wait(srv.submit(r), G)
+        q = po.partition(small_states.energy, small_states.g, T)
+        j = job_init(capi.CONV_PHYSICAL, prof, T, P, q, mass, nu0, d, G, cutoff=25.0)
+        Lh = L if prof == capi.VOIGT else {k: v for k, v in L.items() if k not in ("gamma", "n")}
+        ref = H.oracle_of(j, Lh)
+        if prec == capi.FP64:
+            # Q(T) comes from the device's tree reduction: 1e-12 relative
+            floor = 1e-290 if prof == capi.DOPPLER else 0.0
+            d_ = np.abs(out - ref)
+            assert np.all(d_ <= 1e-10 * np.abs(ref) + floor)
+        else:
+            rel, band = H.fp32_errors(out, ref)
+            assert rel <= H.FP32_REL and band <= H.FP32_BAND
+
+
+def test_admission_by_budget(small_states, small_lines):
+    line_bytes = sum(v.nbytes for v in small_lines.values()) + small_states.energy.nbytes * 2
+    G = 200000
+    budget = line_bytes + 3 * G * 8 + 4096      # room for three outputs at a time
+    srv = Server(0, hbm_budget=budget, streams=2)
+    try:
+        lid = srv.add_list(small_lines, small_states.energy, small_states.g, 18.0)
+        too_big = Server.request(lid, capi.VOIGT, 1000.0, 1.0, 100.0, 0.01, 10 * G)
+        st, _ = srv.try_submit(too_big)
+        assert st == capi.GEXS_ERR_ADMISSION
+        reqs = [Server.request(lid, capi.VOIGT, 300.0 + 100 * i, 1.0, 100.0 + 50 * i, 0.02, G)
+                for i in range(8)]
+        tickets = [srv.submit(r) for r in reqs]
+        peak = [0]
+        done = threading.Event()
+
+        def watch():
+            while not done.is_set():
+                peak[0] = max(peak[0], srv.stats()["inflight_bytes"])
+        th = threading.Thread(target=watch)
+        th.start()
+        outs = [srv.wait(t, G)[0] for t in tickets]
+        done.set()
+        th.join()
+        assert peak[0] <= 3 * G * 8
+        assert all(np.max(o) > 0 for o in outs)
+        st = srv.stats()
+        assert st["submitted"] == st["completed"] == 8
+    finally:
+        srv.close()
+
+
+def test_wait_timeout_and_bad_requests(served):
+    srv, lid, lid_dop = served
+    r = Server.request(lid, capi.VOIGT, 1500.0, 1.0, 100.0, 0.001, 3000000)
+    t = srv.submit(r)
+    st = srv.wait_status(t, 0)
+    assert st in (capi.GEXS_ERR_TIMEOUT, 0)
+    if st == capi.GEXS_ERR_TIMEOUT:
+        srv.wait(t, r.grid_points)
+    bad = Server.request(99, capi.VOIGT, 1500.0, 1.0, 100.0, 0.01, 1000)
+    assert srv.try_submit(bad)[0] == capi.GEXS_ERR_INVALID
+    no_broadening = Server.request(lid_dop, capi.VOIGT, 1500.0, 1.0, 100.0, 0.01, 1000)
+    assert srv.try_submit(no_broadening)[0] == capi.GEXS_ERR_INVALID
