@@ -274,6 +274,113 @@ def batch64(ctx, torch, dev):
                       "0.005": int(np.sum(dnus == 0.005))}}
 
 
+def serve_bench(torch, dev, local_rank, args):
+    """Request loop under Poisson arrivals: three resident synthetic lists
+    (1e7, 1e8, 5e8 lines; 18, 16, 44 amu), requests with T log-uniform
+    100-3000 K, P log-uniform 1e-6-100 bar, resolution log-uniform
+    0.001-0.1 cm^-1, 1e4-1e7 points inside 100-20000 cm^-1, Doppler or
+    Voigt (FP32 form).  Rates are set relative to the measured mean service
+    time; latency = result in the caller's buffer minus submission."""
+    import threading
+    from gexs_b200 import synth, _capi as capi
+    from gexs_b200.engine import Server, Context, Job, LineList
+    scale = args.serve_scale
+    specs = [(int(1e7 * scale), 18.0, 1), (int(1e8 * scale), 16.0, 2), (int(5e8 * scale), 44.0, 3)]
+    srv = Server(local_rank, hbm_budget=0, streams=4)
+    keep, lists = [], []
+    t_gen = time.perf_counter()
+    for n, mass, k in specs:
+        big = n >= int(5e8 * scale)
+        st = synth.make_states(1000000 if big else 200000, 120 if big else 80, 1010 + k)
+        L = synth.make_lines_torch(st, n, NU0, NU1, 2010 + k, broadening_seed=3010 + k, device=dev)
+        lid = srv.add_list(L, st.energy, st.g, mass)
+        keep.append(LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev))
+        lists.append((lid, mass, n))
+        del L
+        torch.cuda.empty_cache()
+    t_gen = time.perf_counter() - t_gen
+    rng = np.random.Generator(np.random.PCG64(4000))
+
+    def draw():
+        li = int(rng.integers(0, 3))
+        T = float(10 ** rng.uniform(2.0, np.log10(3000.0)))
+        P = float(10 ** rng.uniform(-6.0, 2.0))
+        d = float(10 ** rng.uniform(-3.0, -1.0))
+        G = int(10 ** rng.uniform(4.0, 7.0))
+        G = min(G, int(19900.0 / d))
+        nu0 = float(rng.uniform(100.0, 20000.0 - G * d))
+        prof = capi.VOIGT if rng.random() < 0.5 else capi.DOPPLER
+        return li, Server.request(lists[li][0], prof, T, P, nu0, d, G, precision=capi.FP32,
+                                  cutoff=CUT)
+
+    def run(reqs, rate):
+        lat, infos = [None] * len(reqs), [None] * len(reqs)
+        tickets = [None] * len(reqs)
+        ready = [threading.Event() for _ in reqs]
+
+        def client():
+            r2 = np.random.Generator(np.random.PCG64(4100))
+            for i, (_, rq) in enumerate(reqs):
+                if rate:
+                    time.sleep(float(r2.exponential(1.0 / rate)))
+                tickets[i] = srv.submit(rq)
+                ready[i].set()
+        th = threading.Thread(target=client)
+        t0 = time.perf_counter()
+        th.start()
+        for i, (_, rq) in enumerate(reqs):
+            ready[i].wait()
+            out, info = srv.wait(tickets[i], rq.grid_points)
+            lat[i] = info.fetched_ms - info.submit_ms
+            infos[i] = info
+        th.join()
+        return time.perf_counter() - t0, lat, infos
+
+    ctx = Context(local_rank)
+
+    def evals_of(reqs):
+        tot = 0
+        for li, rq in reqs:
+            j = Job(keep[li], torch.empty(1, dtype=torch.float64, device=dev),
+                    convention=capi.CONV_PHYSICAL, profile=rq.profile,
+                    temperature=rq.temperature, pressure=rq.pressure, partition=1.0,
+                    mass=lists[li][1], nu_start=rq.nu_start, dnu=rq.dnu,
+                    grid_points=rq.grid_points, cutoff=CUT, n_points=rq.grid_points)
+            tot += ctx.count_evals([j])[0]
+        return tot
+
+    warm = [draw() for _ in range(3)]
+    run(warm, 0.0)
+    calib = [draw() for _ in range(8)]
+    wall, lat, _ = run([(li, rq) for li, rq in calib], 0.0)
+    # serial service time: run them one by one
+    t0 = time.perf_counter()
+    for li, rq in calib:
+        srv.wait(srv.submit(rq), rq.grid_points)
+    service = (time.perf_counter() - t0) / len(calib)
+    rates = []
+    for load in args.serve_loads:
+        reqs = [draw() for _ in range(args.serve_requests)]
+        rate = load / service
+        wall, lat, infos = run(reqs, rate)
+        ev = evals_of(reqs)
+        lat = np.array(lat)
+        rates.append({"offered_load": load, "rate_per_s": rate, "requests": len(reqs),
+                      "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)),
+                      "mean_ms": float(lat.mean()), "throughput_req_per_s": len(reqs) / wall,
+                      "evals_per_s": ev / wall,
+                      "mean_batch": float(np.mean([i.batch_size for i in infos])),
+                      "max_batch": int(max(i.batch_size for i in infos))})
+    stats = srv.stats()
+    srv.close()
+    return {"lists": [{"lines": n, "mass_amu": m} for _, m, n in lists],
+            "list_generation_s": t_gen, "serial_service_ms": 1e3 * service,
+            "rates": rates, "batches": stats["batches"],
+            "requests": "T log-U(100,3000) K, P log-U(1e-6,100) bar, dnu log-U(0.001,0.1), "
+                        "1e4-1e7 points in 100-20000 cm^-1, Doppler|Voigt, FP32 form"}
+
+
 def e2e_manager(torch, dev, L, q, steps, warmup, local_rank):
     """Same workload through the drop-in manager's C ABI with host buffers."""
     from gexs_b200 import _capi as capi
@@ -435,6 +542,10 @@ def our_arm(args):
         }
     if not args.no_batch and rank == 0:
         result["batch64"] = batch64(ctx, torch, dev)
+    if not args.no_serve and rank == 0:
+        del lines, job, out, L
+        torch.cuda.empty_cache()
+        result["serve"] = serve_bench(torch, dev, local_rank, args)
     if not args.no_cpu and rank == 0 and ws == 1:
         v, cores, sample, kind = cpu_reference_sample(target_s=args.cpu_seconds)
         result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
@@ -456,6 +567,11 @@ def main():
     ap.add_argument("--lines", type=int, default=100_000_000)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-scale", type=float, default=1.0,
+                    help="scale of the three resident line lists (1 = 1e7, 1e8, 5e8 lines)")
+    ap.add_argument("--serve-requests", type=int, default=30)
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.9, 1.5])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--cfg", default="4,4,0",
                     help="launch shape bins_per_lane,warps,ctas_per_sm of the timed kernel")

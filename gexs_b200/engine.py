@@ -276,16 +276,25 @@ class Server:
     def _p(a):
         return None if a is None else a.ctypes.data_as(C.c_void_p)
 
+    @staticmethod
+    def _any(a):
+        if a is None:
+            return None
+        if hasattr(a, "data_ptr"):
+            return C.c_void_p(a.data_ptr())
+        return a.ctypes.data_as(C.c_void_p)
+
     def add_list(self, lines, state_energy, state_g, mass):
-        """lines: dict of host numpy arrays (nu, elow, aif, gns[, gamma, n])."""
+        """lines: dict of arrays nu, elow, aif, gns[, gamma, n] (numpy host
+        arrays or contiguous torch tensors, host or device)."""
         lid = C.c_int()
         se = np.ascontiguousarray(state_energy, dtype=np.float64)
         sg = np.ascontiguousarray(state_g, dtype=np.int32)
+        a = self._any
         check(lib().gexs_server_add_list(
-            self.h, self._p(lines["nu"]), self._p(lines["elow"]), self._p(lines["aif"]),
-            self._p(lines["gns"]), self._p(lines.get("gamma")), self._p(lines.get("n")),
-            len(lines["nu"]), self._p(se), self._p(sg), len(se), float(mass), C.byref(lid)),
-            "gexs_server_add_list")
+            self.h, a(lines["nu"]), a(lines["elow"]), a(lines["aif"]), a(lines["gns"]),
+            a(lines.get("gamma")), a(lines.get("n")), int(lines["nu"].shape[0]), a(se), a(sg),
+            len(se), float(mass), C.byref(lid)), "gexs_server_add_list")
         return lid.value
 
     @staticmethod

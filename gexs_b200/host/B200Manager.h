@@ -23,7 +23,12 @@
 #pragma once
 #include <cstddef>
 #include <vector>
+#ifdef GEXS_USE_REFERENCE_BASEMANAGER
+/* compile inside the GEXS tree against its own Managers/BaseManager.h */
+#include <BaseManager.h>
+#else
 #include "BaseManager.h"
+#endif
 #include "../../include/gexs_b200.h"
 
 class B200Manager : public BaseManager {

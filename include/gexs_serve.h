@@ -63,10 +63,11 @@ int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int stre
                        gexs_server** out);
 int gexs_server_destroy(gexs_server* s);
 
-/* Upload a line list (sorted by nu) and the states used for
- * its Q(T) (energies, degeneracies; host arrays).  gamma / n may be NULL
- * (Doppler and Gaussian requests only).  Fails with GEXS_ERR_ADMISSION
- * when it does not fit in the budget. */
+/* Upload a line list (sorted by nu) and the states used for its Q(T)
+ * (energies, degeneracies).  The arrays may be host or device memory
+ * (copied with cudaMemcpyDefault).  gamma / n may be NULL (Doppler and
+ * Gaussian requests only).  Fails with GEXS_ERR_ADMISSION when the list
+ * does not fit in the budget. */
 int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow,
                          const double* aif, const int32_t* gns, const double* gamma,
                          const double* n, int64_t count, const double* state_energy,
