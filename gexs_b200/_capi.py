@@ -44,7 +44,9 @@ class GexsJob(C.Structure):
 
 class GexsLaunchCfg(C.Structure):
     _fields_ = [("bins_per_lane", C.c_int32), ("warps", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("flags", C.c_int32)]
+
+LAUNCH_DERIVE_ON_LOAD = 1
 
 
 class GexsRequest(C.Structure):

@@ -77,11 +77,13 @@ struct gexs_ctx {
 
 static gexs_launch_cfg default_cfg(int pk, int prec)
 {
+    /* measured best on B200 for the 1e8-line Voigt workload; gexs_autotune
+     * replaces it per (profile, precision) */
     gexs_launch_cfg c;
     c.bins_per_lane = 4;
-    c.warps = 8;
+    c.warps = 4;
     c.ctas_per_sm = 0;
-    c.reserved = 0;
+    c.flags = 0;
     (void)pk; (void)prec;
     return c;
 }
@@ -139,25 +141,64 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
     return GEXS_OK;
 }
 
-/* device image of a group: [jobs][prefix][counter] */
-static size_t group_bytes(const Group& g, size_t* off_prefix, size_t* off_counter)
+/* device image of a group:
+ *   [jobs][prefix][counter][prep pointers][prep arrays (S|invw|y per job)]
+ * prep arrays only when the group derives per job (the default). */
+struct Layout {
+    size_t op, oc, opp, oprep, bytes;
+    std::vector<size_t> job_prep;   /* byte offset of each job's prep arrays */
+};
+
+static Layout group_layout(const Group& g, bool prep)
 {
-    size_t a = g.jobs.size() * sizeof(gexs_job);
-    a = (a + 255) & ~size_t(255);
-    *off_prefix = a;
-    a += g.prefix.size() * sizeof(int);
-    a = (a + 255) & ~size_t(255);
-    *off_counter = a;
-    return a + 256;
+    Layout L;
+    auto up = [](size_t a) { return (a + 255) & ~size_t(255); };
+    size_t a = up(g.jobs.size() * sizeof(gexs_job));
+    L.op = a;
+    a = up(a + g.prefix.size() * sizeof(int));
+    L.oc = a;
+    a += 256;
+    L.opp = a;
+    a = up(a + g.jobs.size() * sizeof(double*));
+    L.oprep = a;
+    for (const gexs_job& j : g.jobs) {
+        L.job_prep.push_back(a);
+        if (prep) a = up(a + (size_t)j.lines.count * 3 * sizeof(double));
+    }
+    L.bytes = a + 256;
+    return L;
 }
 
-static std::vector<unsigned char> group_image(const Group& g, size_t bytes, size_t op, size_t oc)
+static std::vector<unsigned char> group_image(const Group& g, const Layout& L, unsigned char* dev,
+                                              bool prep)
 {
-    std::vector<unsigned char> h(bytes, 0);
+    std::vector<unsigned char> h(L.oprep, 0);
     std::memcpy(h.data(), g.jobs.data(), g.jobs.size() * sizeof(gexs_job));
-    std::memcpy(h.data() + op, g.prefix.data(), g.prefix.size() * sizeof(int));
-    (void)oc;
+    std::memcpy(h.data() + L.op, g.prefix.data(), g.prefix.size() * sizeof(int));
+    double** pp = reinterpret_cast<double**>(h.data() + L.opp);
+    for (size_t i = 0; i < g.jobs.size(); ++i)
+        pp[i] = prep ? reinterpret_cast<double*>(dev + L.job_prep[i]) : nullptr;
     return h;
+}
+
+static int64_t max_lines(const Group& g)
+{
+    int64_t m = 0;
+    for (const gexs_job& j : g.jobs) m = std::max<int64_t>(m, j.lines.count);
+    return m;
+}
+
+/* prep kernel then tile kernel for one group whose image is at d */
+static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char* d, bool prep,
+                                 const gexs_launch_cfg& cfg, int* d_err, int nsm, cudaStream_t s)
+{
+    double* const* pp = reinterpret_cast<double* const*>(d + L.opp);
+    cudaError_t e = cudaSuccess;
+    if (prep) e = launch_prep((const gexs_job*)d, pp, (int)g.jobs.size(), max_lines(g), nsm, s);
+    if (e != cudaSuccess) return e;
+    return launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + L.op),
+                        (int)g.jobs.size(), g.nitems, (int*)(d + L.oc), d_err,
+                        prep ? pp : nullptr, cfg, nsm, s);
 }
 
 extern "C" {
@@ -309,17 +350,16 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& g = groups[gi];
         if (g.nitems == 0) continue;
-        size_t op, oc;
-        size_t bytes = group_bytes(g, &op, &oc);
-        std::vector<unsigned char> h = group_image(g, bytes, op, oc);
+        const bool prep = !(cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
+        Layout L = group_layout(g, prep);
         void* d = nullptr;
-        e = cudaMallocAsync(&d, bytes, s);
+        e = cudaMallocAsync(&d, L.bytes, s);
         if (e != cudaSuccess) return set_error(GEXS_ERR_OOM, "launch tables");
-        e = cudaMemcpyAsync(d, h.data(), bytes, cudaMemcpyHostToDevice, s);
+        std::vector<unsigned char> h = group_image(g, L, (unsigned char*)d, prep);
+        e = cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync((unsigned char*)d + L.oc, 0, sizeof(int), s);
         if (e != cudaSuccess) { cudaFreeAsync(d, s); return cuda_error(e, "upload launch tables"); }
-        unsigned char* b = (unsigned char*)d;
-        e = launch_tiles(g.pk, g.prec, (const gexs_job*)b, (const int*)(b + op), (int)g.jobs.size(),
-                         g.nitems, (int*)(b + oc), ctx->d_err, cfgs[gi], ctx->nsm, s);
+        e = enqueue_group(g, L, (unsigned char*)d, prep, cfgs[gi], ctx->d_err, ctx->nsm, s);
         cudaFreeAsync(d, s);
         if (e != cudaSuccess) return cuda_error(e, "tile kernel launch");
     }
@@ -358,7 +398,8 @@ struct gexs_batch {
     std::vector<Group> groups;
     std::vector<gexs_launch_cfg> cfgs;
     std::vector<void*> dmem;          /* per group device image */
-    std::vector<size_t> op, oc;
+    std::vector<Layout> layouts;
+    std::vector<bool> prep;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -369,11 +410,10 @@ static int batch_enqueue(gexs_batch* b, cudaStream_t s)
         const Group& g = b->groups[gi];
         if (g.nitems == 0) continue;
         unsigned char* d = (unsigned char*)b->dmem[gi];
-        cudaError_t e = cudaMemsetAsync(d + b->oc[gi], 0, sizeof(int), s);
+        cudaError_t e = cudaMemsetAsync(d + b->layouts[gi].oc, 0, sizeof(int), s);
         if (e != cudaSuccess) return cuda_error(e, "reset work counter");
-        e = launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + b->op[gi]),
-                         (int)g.jobs.size(), g.nitems, (int*)(d + b->oc[gi]), b->ctx->d_err,
-                         b->cfgs[gi], b->ctx->nsm, s);
+        e = enqueue_group(g, b->layouts[gi], d, b->prep[gi], b->cfgs[gi], b->ctx->d_err,
+                          b->ctx->nsm, s);
         if (e != cudaSuccess) return cuda_error(e, "tile kernel launch");
     }
     return GEXS_OK;
@@ -391,14 +431,15 @@ int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
     b->ctx = ctx;
     int st = build_groups(jobs, njobs, cfg, ctx, b->groups, b->cfgs);
     if (st) { delete b; return st; }
-    for (const Group& g : b->groups) {
-        size_t op, oc;
-        size_t bytes = group_bytes(g, &op, &oc);
-        std::vector<unsigned char> h = group_image(g, bytes, op, oc);
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const Group& g = b->groups[gi];
+        const bool prep = !(b->cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
+        Layout L = group_layout(g, prep);
         void* d = nullptr;
-        if (cudaMalloc(&d, bytes) != cudaSuccess) { gexs_batch_destroy(b); return set_error(GEXS_ERR_OOM, "batch tables"); }
-        b->dmem.push_back(d); b->op.push_back(op); b->oc.push_back(oc);
-        cudaError_t e = cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice);
+        if (cudaMalloc(&d, L.bytes) != cudaSuccess) { gexs_batch_destroy(b); return set_error(GEXS_ERR_OOM, "batch tables"); }
+        b->dmem.push_back(d); b->layouts.push_back(L); b->prep.push_back(prep);
+        std::vector<unsigned char> h = group_image(g, L, (unsigned char*)d, prep);
+        cudaError_t e = cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { gexs_batch_destroy(b); return cuda_error(e, "upload batch tables"); }
     }
     *out = b;
@@ -475,7 +516,7 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
     for (int bi = 0; bi < 3 && !st; ++bi)
         for (int wi = 0; wi < 2 && !st; ++wi) {
             gexs_launch_cfg c; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
-            c.ctas_per_sm = 0; c.reserved = 0;
+            c.ctas_per_sm = 0; c.flags = 0;
             gexs_batch* b = nullptr;
             st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);
             if (st) break;

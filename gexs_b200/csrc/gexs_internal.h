@@ -10,9 +10,14 @@ namespace gexs {
 /* kernel launchers (gexs_kernels.cu) */
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
+/* d_prep: device array of per-job prep arrays (S | invw | y, 3 N doubles
+ * each, from launch_prep), or NULL to derive every line on load */
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
-                         const gexs_launch_cfg& cfg, int nsm, cudaStream_t st);
+                         double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
+                         cudaStream_t st);
+cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs,
+                        int64_t max_lines, int nsm, cudaStream_t st);
 cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,
                          int nsm, cudaStream_t st);
 cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,

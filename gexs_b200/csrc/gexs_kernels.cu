@@ -21,6 +21,7 @@
  *  - FP32 form: per-stage FP32 partial sums merged into a Kahan-compensated
  *    (sum, compensation) pair per bin; FP64 form: plain FP64 sums.
  */
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
@@ -193,17 +194,23 @@ __device__ __forceinline__ int centered(const Tile& T, int wa, int wb, double nu
 /* ------------------------------------------------------------ derive one line */
 struct RawLine { double nu, elow, aif, gam, nexp; int g; };
 
+/* FP64 per-line quantities of a job: centre (after the nu==0 rule), S(T),
+ * 1/width and y = gammaL/width.  Either computed on load or read from the
+ * job's prep arrays (prep_kernel). */
+struct LineQ { double nu, S, invw, y; };
+
 template <int PK>
 struct Derived {
     double nu, S, invw, y, tc;
     int win, c1, c2, c3;
 };
 
-template <int PK>
-__device__ __noinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L, double zthr)
+/* S(T) (Managers/CPU/OpenMPManager.cpp:394-396 operation order), the width
+ * and y (:398,404) */
+template <bool PRESS>
+__device__ __forceinline__ LineQ line_quantities(const gexs_job& J, const RawLine& L)
 {
-    const gexs_job& J = *T.J;
-    Derived<PK> d;
+    LineQ q;
     double nu = L.nu == 0.0 ? 1e-6 : L.nu;
     double t = dmul(J.s_scale, L.aif);
     t = dmul(t, (double)L.g);
@@ -211,16 +218,27 @@ __device__ __noinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L,
     t = dmul(t, exp(dmul(-J.beta, L.elow)));
     t = dmul(t, dsub(1.0, exp(dmul(-J.beta, nu))));
     double den = dmul(dmul(nu, nu), J.partition);
-    d.nu = nu;
-    d.S = ddiv(t, den);
-    d.invw = (J.profile == GEXS_GAUSSIAN) ? J.inv_width : ddiv(1.0, dmul(nu, J.dop_coef));
-    if constexpr (PK != PK_ERF) {
+    q.nu = nu;
+    q.S = ddiv(t, den);
+    q.invw = (J.profile == GEXS_GAUSSIAN) ? J.inv_width : ddiv(1.0, dmul(nu, J.dop_coef));
+    if constexpr (PRESS) {
         double gl = dmul(L.gam, pow(J.t_ratio, L.nexp));
         gl = dmul(gl, J.gamma_scale);
-        d.y = dmul(gl, d.invw);
+        q.y = dmul(gl, q.invw);
     } else {
-        d.y = 0.0;
+        q.y = 0.0;
     }
+    return q;
+}
+
+/* tile-dependent part: centre in bins, window and Humlicek region limits */
+template <int PK>
+__device__ __noinline__ Derived<PK> derive_line(const Tile& T, const LineQ& q, double zthr)
+{
+    const gexs_job& J = *T.J;
+    Derived<PK> d;
+    const double nu = q.nu;
+    d.nu = nu; d.S = q.S; d.invw = q.invw; d.y = q.y;
     d.tc = ddiv(dsub(nu, T.f0), J.dnu);
     int a, b;
     tile_window(T, nu, d.tc, &a, &b);
@@ -254,6 +272,36 @@ __device__ __noinline__ Derived<PK> derive_line(const Tile& T, const RawLine& L,
     return d;
 }
 
+/* ------------------------------------------------------------ prep kernel
+ * Per job, the FP64 per-line quantities once: S at base[i], invw at
+ * base[N + i], y at base[2N + i] (N = line count).  The tile kernel then
+ * reads 32 bytes per line instead of recomputing two exponentials, a power
+ * and two divisions for every tile the line reaches. */
+__global__ void prep_kernel(const gexs_job* __restrict__ jobs, double* const* __restrict__ prep)
+{
+    const gexs_job& J = jobs[blockIdx.y];
+    double* base = prep[blockIdx.y];
+    const int64_t N = J.lines.count;
+    const bool press = J.profile == GEXS_VOIGT || J.profile == GEXS_VOIGT_QUAD;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        RawLine L;
+        L.nu = J.lines.nu[i]; L.elow = J.lines.elow[i]; L.aif = J.lines.aif[i];
+        L.g = J.lines.gns[i];
+        LineQ q;
+        if (press) {
+            L.gam = J.lines.gamma[i]; L.nexp = J.lines.n[i];
+            q = line_quantities<true>(J, L);
+        } else {
+            L.gam = 0.0; L.nexp = 0.0;
+            q = line_quantities<false>(J, L);
+        }
+        base[i] = q.S;
+        base[N + i] = q.invw;
+        base[2 * N + i] = q.y;
+    }
+}
+
 /* ------------------------------------------------------------ kernel args */
 struct KArgs {
     const gexs_job* jobs;
@@ -262,6 +310,7 @@ struct KArgs {
     int             nitems;
     int*            counter;   /* work counter (zeroed before launch)    */
     int*            err;       /* sticky error word                      */
+    double* const*  prep;      /* per job S|invw|y arrays, or NULL       */
 };
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
@@ -557,7 +606,7 @@ __device__ __forceinline__ void lines_f64(const RecF64* __restrict__ rec, int nr
 }
 
 /* shared-memory layout of one CTA (dynamic shared memory) */
-template <int PK, int PREC, int B, int WARPS>
+template <int PK, int PREC, int B, int WARPS, bool PREP>
 struct Smem {
     static constexpr int NT = WARPS * 32;
     static constexpr int W = 32 * B * WARPS;
@@ -565,13 +614,10 @@ struct Smem {
     static constexpr bool PRESS = (PK != PK_ERF);
     static constexpr bool CORE = (PREC == GEXS_FP32 && PK == PK_VOIGT);
     static constexpr size_t raw_d = (size_t)2 * NT * sizeof(double);   /* one f64 array, 2 bufs */
-    static constexpr size_t off_nu = 0;
-    static constexpr size_t off_el = off_nu + raw_d;
-    static constexpr size_t off_ai = off_el + raw_d;
-    static constexpr size_t off_ga = off_ai + raw_d;
-    static constexpr size_t off_ne = off_ga + (PRESS ? raw_d : 0);
-    static constexpr size_t off_gn = off_ne + (PRESS ? raw_d : 0);
-    static constexpr size_t off_rec = (off_gn + (size_t)2 * NT * sizeof(int) + 15) & ~size_t(15);
+    /* staged per line: PREP nu S invw y ; on-load nu elow aif [gamma n] gns */
+    static constexpr int NF64 = PREP ? 4 : (PRESS ? 5 : 3);
+    static constexpr size_t off_gn = NF64 * raw_d;
+    static constexpr size_t off_rec = (off_gn + (PREP ? 0 : (size_t)2 * NT * sizeof(int)) + 15) & ~size_t(15);
     static constexpr size_t rec_sz = (PREC == GEXS_FP32) ? sizeof(RecF32) : sizeof(RecF64);
     static constexpr size_t off_core = off_rec + (size_t)R * rec_sz;
     static constexpr size_t off_wacc = (off_core + (CORE ? (size_t)R * sizeof(CoreF64) : 0) + 15) & ~size_t(15);
@@ -583,22 +629,19 @@ struct Smem {
 template <int B, int WARPS>
 constexpr int min_ctas() { return WARPS == 8 ? (B == 8 ? 2 : 3) : (B == 8 ? 4 : 6); }
 
-template <int PK, int PREC, int B, int WARPS>
+template <int PK, int PREC, int B, int WARPS, bool PREP>
 __global__ void __launch_bounds__(WARPS * 32, min_ctas<B, WARPS>())
 tile_kernel(const KArgs args)
 {
-    typedef Smem<PK, PREC, B, WARPS> L;
+    typedef Smem<PK, PREC, B, WARPS, PREP> L;
     constexpr int NT = L::NT;
     constexpr int R = L::R;
     constexpr int W = 32 * B * WARPS;
     typedef typename RecOf<PREC>::T Rec;
 
     extern __shared__ __align__(16) unsigned char smem[];
-    double* s_nu = reinterpret_cast<double*>(smem + L::off_nu);
-    double* s_el = reinterpret_cast<double*>(smem + L::off_el);
-    double* s_ai = reinterpret_cast<double*>(smem + L::off_ai);
-    double* s_ga = reinterpret_cast<double*>(smem + L::off_ga);
-    double* s_ne = reinterpret_cast<double*>(smem + L::off_ne);
+    /* staging arrays f[k][2*NT] (k < NF64) and gns[2*NT] */
+    double* s_f = reinterpret_cast<double*>(smem);
     int*    s_gn = reinterpret_cast<int*>(smem + L::off_gn);
     Rec*    s_rec = reinterpret_cast<Rec*>(smem + L::off_rec);
     CoreF64* s_core = reinterpret_cast<CoreF64*>(smem + L::off_core);
@@ -657,17 +700,25 @@ tile_kernel(const KArgs args)
          * every thread only ever reads the staging slots it filled itself,
          * so the double-buffered cp.async pipeline needs no barrier */
         const int nsub = nph * PH;
+        const double* pb = nullptr;
+        if constexpr (PREP) pb = args.prep[jl];
         auto issue = [&](int u) {
             const int64_t i = lo + (int64_t)u * NT + tid;
             const int o = (u & 1) * NT + tid;
             if (u < nsub && i < hi) {
-                cp_async8(s_nu + o, J.lines.nu + i);
-                cp_async8(s_el + o, J.lines.elow + i);
-                cp_async8(s_ai + o, J.lines.aif + i);
-                cp_async4(s_gn + o, J.lines.gns + i);
-                if constexpr (L::PRESS) {
-                    cp_async8(s_ga + o, J.lines.gamma + i);
-                    cp_async8(s_ne + o, J.lines.n + i);
+                cp_async8(s_f + o, J.lines.nu + i);
+                if constexpr (PREP) {
+                    cp_async8(s_f + 2 * NT + o, pb + i);
+                    cp_async8(s_f + 4 * NT + o, pb + nl + i);
+                    cp_async8(s_f + 6 * NT + o, pb + 2 * nl + i);
+                } else {
+                    cp_async8(s_f + 2 * NT + o, J.lines.elow + i);
+                    cp_async8(s_f + 4 * NT + o, J.lines.aif + i);
+                    cp_async4(s_gn + o, J.lines.gns + i);
+                    if constexpr (L::PRESS) {
+                        cp_async8(s_f + 6 * NT + o, J.lines.gamma + i);
+                        cp_async8(s_f + 8 * NT + o, J.lines.n + i);
+                    }
                 }
             }
             cp_async_commit();
@@ -685,11 +736,20 @@ tile_kernel(const KArgs args)
                 cp_async_wait<1>();
                 const int r = sub * NT + tid;
                 if (r < nrec) {
-                    RawLine Lr;
-                    Lr.nu = s_nu[o]; Lr.elow = s_el[o]; Lr.aif = s_ai[o]; Lr.g = s_gn[o];
-                    if constexpr (L::PRESS) { Lr.gam = s_ga[o]; Lr.nexp = s_ne[o]; }
-                    else { Lr.gam = 0.0; Lr.nexp = 0.0; }
-                    Derived<PK> d = derive_line<PK>(T, Lr, zthr);
+                    LineQ lq;
+                    if constexpr (PREP) {
+                        const double nu = s_f[o];
+                        lq.nu = nu == 0.0 ? 1e-6 : nu;
+                        lq.S = s_f[2 * NT + o]; lq.invw = s_f[4 * NT + o]; lq.y = s_f[6 * NT + o];
+                    } else {
+                        RawLine Lr;
+                        Lr.nu = s_f[o]; Lr.elow = s_f[2 * NT + o]; Lr.aif = s_f[4 * NT + o];
+                        Lr.g = s_gn[o];
+                        if constexpr (L::PRESS) { Lr.gam = s_f[6 * NT + o]; Lr.nexp = s_f[8 * NT + o]; }
+                        else { Lr.gam = 0.0; Lr.nexp = 0.0; }
+                        lq = line_quantities<L::PRESS>(J, Lr);
+                    }
+                    Derived<PK> d = derive_line<PK>(T, lq, zthr);
                     Rec rr;
                     make_rec<PK, B, WARPS>(rr, d, J, T);
                     s_rec[r] = rr;
@@ -810,11 +870,11 @@ __global__ void partition_final(const double* partial, int nchunk, int nt, doubl
 }
 
 /* ------------------------------------------------------------ dispatch */
-template <int PK, int PREC, int B, int WARPS>
+template <int PK, int PREC, int B, int WARPS, bool PREP>
 static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st)
 {
-    auto kern = tile_kernel<PK, PREC, B, WARPS>;
-    const size_t smem = Smem<PK, PREC, B, WARPS>::bytes;
+    auto kern = tile_kernel<PK, PREC, B, WARPS, PREP>;
+    const size_t smem = Smem<PK, PREC, B, WARPS, PREP>::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
@@ -828,17 +888,39 @@ static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStre
     return cudaGetLastError();
 }
 
-template <int PK, int PREC>
+template <int PK, int PREC, bool PREP>
 static cudaError_t launch_cfg(const KArgs& a, const gexs_launch_cfg& c, int nsm, cudaStream_t st)
 {
     if (c.warps == 8) {
-        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 8>(a, c.ctas_per_sm, nsm, st);
-        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 8>(a, c.ctas_per_sm, nsm, st);
-        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 8>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 8, PREP>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 8, PREP>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 8, PREP>(a, c.ctas_per_sm, nsm, st);
     } else if (c.warps == 4) {
-        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 4>(a, c.ctas_per_sm, nsm, st);
-        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 4>(a, c.ctas_per_sm, nsm, st);
-        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 4>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 8) return launch_one<PK, PREC, 8, 4, PREP>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 4) return launch_one<PK, PREC, 4, 4, PREP>(a, c.ctas_per_sm, nsm, st);
+        if (c.bins_per_lane == 2) return launch_one<PK, PREC, 2, 4, PREP>(a, c.ctas_per_sm, nsm, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <bool PREP>
+static cudaError_t launch_prec(int pk, int prec, const KArgs& a, const gexs_launch_cfg& cfg,
+                               int nsm, cudaStream_t st)
+{
+    if (prec == GEXS_FP32) {
+        switch (pk) {
+        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP32, PREP>(a, cfg, nsm, st);
+        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP32, PREP>(a, cfg, nsm, st);
+        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP32, PREP>(a, cfg, nsm, st);
+        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP32, PREP>(a, cfg, nsm, st);
+        }
+    } else {
+        switch (pk) {
+        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP64, PREP>(a, cfg, nsm, st);
+        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP64, PREP>(a, cfg, nsm, st);
+        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP64, PREP>(a, cfg, nsm, st);
+        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP64, PREP>(a, cfg, nsm, st);
+        }
     }
     return cudaErrorInvalidValue;
 }
@@ -853,27 +935,24 @@ int profile_class(const gexs_job& j)
 
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
-                         const gexs_launch_cfg& cfg, int nsm, cudaStream_t st)
+                         double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
+                         cudaStream_t st)
 {
     KArgs a;
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
-    a.counter = d_counter; a.err = d_err;
-    if (prec == GEXS_FP32) {
-        switch (pk) {
-        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP32>(a, cfg, nsm, st);
-        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP32>(a, cfg, nsm, st);
-        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP32>(a, cfg, nsm, st);
-        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP32>(a, cfg, nsm, st);
-        }
-    } else {
-        switch (pk) {
-        case PK_VOIGT: return launch_cfg<PK_VOIGT, GEXS_FP64>(a, cfg, nsm, st);
-        case PK_ERF:   return launch_cfg<PK_ERF, GEXS_FP64>(a, cfg, nsm, st);
-        case PK_GH16:  return launch_cfg<PK_GH16, GEXS_FP64>(a, cfg, nsm, st);
-        case PK_GH32:  return launch_cfg<PK_GH32, GEXS_FP64>(a, cfg, nsm, st);
-        }
-    }
-    return cudaErrorInvalidValue;
+    a.counter = d_counter; a.err = d_err; a.prep = d_prep;
+    return d_prep ? launch_prec<true>(pk, prec, a, cfg, nsm, st)
+                  : launch_prec<false>(pk, prec, a, cfg, nsm, st);
+}
+
+cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs,
+                        int64_t max_lines, int nsm, cudaStream_t st)
+{
+    if (max_lines <= 0) return cudaSuccess;
+    int bx = (int)std::min<int64_t>((max_lines + 255) / 256, (int64_t)nsm * 8);
+    dim3 grid(bx, njobs);
+    prep_kernel<<<grid, 256, 0, st>>>(d_jobs, d_prep);
+    return cudaGetLastError();
 }
 
 int tile_bins(const gexs_launch_cfg& c) { return 32 * c.bins_per_lane * c.warps; }

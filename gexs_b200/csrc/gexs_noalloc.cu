@@ -64,7 +64,7 @@ extern "C" int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_laun
         return set_error(GEXS_ERR_INVALID, "gexs_run_noalloc: njobs must be 1.." +
                                                std::to_string(GEXS_NOALLOC_MAX_JOBS));
     gexs_launch_cfg c;
-    c.bins_per_lane = 4; c.warps = 8; c.ctas_per_sm = 0; c.reserved = 0;
+    c.bins_per_lane = 4; c.warps = 8; c.ctas_per_sm = 0; c.flags = GEXS_LAUNCH_DERIVE_ON_LOAD;
     if (cfg) c = *cfg;
     if (!((c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8) &&
           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0))
@@ -112,7 +112,8 @@ extern "C" int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_laun
     if (e == cudaSuccess) e = cudaMemsetAsync(base + kCounterOff, 0, sizeof(int), s);
     if (e != cudaSuccess) return cuda_error(e, "gexs_run_noalloc: upload launch tables");
     e = launch_tiles(pk, prec, (const gexs_job*)base, (const int*)(base + kPrefixOff), njobs,
-                     (int)nitems, (int*)(base + kCounterOff), (int*)(base + kErrOff), c, nsm, s);
+                     (int)nitems, (int*)(base + kCounterOff), (int*)(base + kErrOff), nullptr, c, nsm,
+                     s);
     if (e != cudaSuccess) return cuda_error(e, "gexs_run_noalloc: tile kernel launch");
     return GEXS_OK;
 }

@@ -109,8 +109,8 @@ def _cfg(cfg):
         return None
     if isinstance(cfg, capi.GexsLaunchCfg):
         return C.byref(cfg)
-    b, w, c = cfg
-    return C.byref(capi.GexsLaunchCfg(b, w, c, 0))
+    b, w, c = cfg[:3]
+    return C.byref(capi.GexsLaunchCfg(b, w, c, cfg[3] if len(cfg) > 3 else 0))
 
 
 class Batch:

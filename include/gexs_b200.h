@@ -150,11 +150,15 @@ int gexs_job_init(gexs_job* job, int convention, int profile,
 typedef struct gexs_ctx gexs_ctx;
 
 typedef struct gexs_launch_cfg {
-    int32_t bins_per_lane;   /* 2, 4 or 8                       */
-    int32_t warps;           /* 4 or 8 (tile = 32*bins*warps)   */
-    int32_t ctas_per_sm;     /* resident CTAs per SM (>=1)      */
-    int32_t reserved;
+    int32_t bins_per_lane;   /* 2, 4 or 8                            */
+    int32_t warps;           /* 4 or 8 (tile = 32*bins*warps)        */
+    int32_t ctas_per_sm;     /* resident CTAs per SM (0 = max)       */
+    int32_t flags;           /* GEXS_LAUNCH_*                        */
 } gexs_launch_cfg;
+
+/* derive S(T), width and y of every line in the tile loader instead of
+ * once per job by a prep kernel (no per-job scratch of 24 B per line) */
+#define GEXS_LAUNCH_DERIVE_ON_LOAD 1
 
 int         gexs_ctx_create(int device, gexs_ctx** out);
 int         gexs_ctx_destroy(gexs_ctx* ctx);

@@ -207,3 +207,16 @@ def test_fp32_narrow_and_broad_lines(gpu_ctx, small_lines, T, P, dnu):
         job = _make(small_lines, capi.FP32, prof, 16, capi.CONV_PHYSICAL, T=T, P=P, dnu=dnu, G=G,
                     cutoff=25.0)
         _check(gpu_ctx, job, small_lines)
+
+
+@pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
+@pytest.mark.parametrize("profile", [capi.VOIGT, capi.DOPPLER])
+def test_prep_and_on_load_paths_agree_bitwise(gpu_ctx, small_lines, prec, profile):
+    """Per-job prep of S(T), width and y (default) and derive-on-load give
+    the same doubles, so the results are identical."""
+    a = _make(small_lines, prec, profile, 16, capi.CONV_PHYSICAL, T=800.0, P=0.2)
+    b = _make(small_lines, prec, profile, 16, capi.CONV_PHYSICAL, T=800.0, P=0.2)
+    gpu_ctx.run([a], cfg=(4, 8, 0, 0))
+    gpu_ctx.run([b], cfg=(4, 8, 0, capi.LAUNCH_DERIVE_ON_LOAD))
+    gpu_ctx.check()
+    assert torch.equal(a.out, b.out)
