@@ -62,6 +62,12 @@ __device__ __forceinline__ R re_div(R nr, R ni, R dr, R di)
 {
     return (nr * dr + ni * di) / (dr * dr + di * di);
 }
+/* FP32: one approximate reciprocal (1 ulp) instead of an IEEE division */
+template <>
+__device__ __forceinline__ float re_div<float>(float nr, float ni, float dr, float di)
+{
+    return fmaf(nr, dr, ni * di) * rcp_approx(fmaf(dr, dr, di * di));
+}
 
 template <typename R>
 __device__ __forceinline__ R hum_region2(R x, R y)

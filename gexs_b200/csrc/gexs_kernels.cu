@@ -454,26 +454,34 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec,
             }
             /* general tier: window edges and region-I bins of warps that
              * hold part of the core; the core bins themselves are left to
-             * core_pass_f32 */
+             * core_pass_f32.  Every bin is evaluated and the accumulation
+             * is predicated, so the warp does not diverge. */
             const int a = lo16(qi.x), b = hi16(qi.x);
             const int c1a = lo16(qi.y), c1b = hi16(qi.y);
-            const bool wide = (mask >> 24) & 1;
+            if (!((mask >> 24) & 1)) {
 #pragma unroll
-            for (int k = 0; k < B; ++k) {
-                const int t = wb + lane + 32 * k;
-                if (t < a || t >= b || (t >= c1a && t < c1b)) continue;
-                const float x = fabsf(((t0 + (float)(32 * k)) - q1.w) * q0.y);
-                const float x2 = x * x;
-                const float num = x2 + q1.x;
-                float v;
-                if (!wide) {
+                for (int k = 0; k < B; ++k) {
+                    const int t = wb + lane + 32 * k;
+                    const float x = ((t0 + (float)(32 * k)) - q1.w) * q0.y;
+                    const float x2 = x * x;
+                    const float num = x2 + q1.x;
                     const float den = fmaf(x2, -2.f, num * num);
-                    v = num * rcp_approx(den) * q0.w;
-                } else {
-                    /* num/den = 1/(num - 2 x^2/num) without num^2 */
-                    v = (x < 1e18f) ? q0.w / (num - 2.f * (x2 / num)) : 0.f;
+                    const float v = num * rcp_approx(den) * q0.w;
+                    const bool in = (unsigned)(t - a) < (unsigned)(b - a) &&
+                                    !((unsigned)(t - c1a) < (unsigned)(c1b - c1a));
+                    part[k] += in ? v : 0.f;
                 }
-                part[k] += v;
+            } else {
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = wb + lane + 32 * k;
+                    if (t < a || t >= b || (t >= c1a && t < c1b)) continue;
+                    const float x = fabsf(((t0 + (float)(32 * k)) - q1.w) * q0.y);
+                    const float x2 = x * x;
+                    const float num = x2 + q1.x;
+                    /* num/den = 1/(num - 2 x^2/num) without num^2 */
+                    part[k] += (x < 1e18f) ? q0.w / (num - 2.f * (x2 / num)) : 0.f;
+                }
             }
         } else if constexpr (PK == PK_ERF) {
             const int a = lo16(qi.x), b = hi16(qi.x);
@@ -531,19 +539,30 @@ __device__ __forceinline__ void core_pass_f32(const RecF32* __restrict__ rec,
         const int c1 = rec[i].c1;
         const int c1a = lo16(c1), c1b = hi16(c1);
         if (c1a >= c1b) continue;
+        /* the core as contiguous single-region ranges, in a fixed order:
+         * II [c1a, c2a) | IV [c2a, c3a) | III [c3a, c3b) | IV [c3b, c2b) |
+         * II [c2b, c1b), c3 within c2 within c1 (empty ranges skipped) */
+        const int c2 = core[i].c2, c3 = core[i].c3;
+        int c2a = lo16(c2), c2b = hi16(c2);
+        if (c2a >= c2b) c2a = c2b = c1b;
+        int c3a = lo16(c3), c3b = hi16(c3);
+        if (c3a >= c3b) c3a = c3b = c2b;
+        const int lo[5] = {c1a, c2a, c3a, c3b, c2b};
+        const int hi[5] = {c2a, c3a, c3b, c2b, c1b};
+        const int rg[5] = {2, 4, 3, 4, 2};
         const float icf = rec[i].icf, fc = rec[i].fc, dx = rec[i].dx, y = rec[i].y;
         const float amp = rec[i].amp;
-        const int c2 = core[i].c2, c3 = core[i].c3;
-        for (int t = c1a + lane; t < c1b; t += 32) {
-            float v;
-            if (t < lo16(c2) || t >= hi16(c2)) {
-                const float x = fabsf(((float)t - icf) - fc) * dx;
-                v = amp * hum_region2<float>(x, y);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            if (rg[r] == 2) {
+                for (int t = lo[r] + lane; t < hi[r]; t += 32) {
+                    const float x = fabsf(((float)t - icf) - fc) * dx;
+                    wacc[t] += amp * hum_region2<float>(x, y);
+                }
             } else {
-                const int reg = (t >= lo16(c3) && t < hi16(c3)) ? 3 : 4;
-                v = core_term_f64(reg, grid_f(nu_start, dnu, j0 + t), core[i]);
+                for (int t = lo[r] + lane; t < hi[r]; t += 32)
+                    wacc[t] += core_term_f64(rg[r], grid_f(nu_start, dnu, j0 + t), core[i]);
             }
-            wacc[t] += v;
         }
     }
 }
