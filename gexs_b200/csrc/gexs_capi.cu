@@ -77,14 +77,15 @@ struct gexs_ctx {
 
 static gexs_launch_cfg default_cfg(int pk, int prec)
 {
-    /* measured best on B200 for the 1e8-line Voigt workload; gexs_autotune
-     * replaces it per (profile, precision) */
+    /* measured best on B200 for the 1e8-line Voigt workload (FP32: 4 bins x
+     * 4 warps, FP64: 4 x 8); gexs_autotune replaces it per (profile,
+     * precision) */
     gexs_launch_cfg c;
     c.bins_per_lane = 4;
-    c.warps = 4;
+    c.warps = (prec == GEXS_FP64) ? 8 : 4;
     c.ctas_per_sm = 0;
     c.flags = 0;
-    (void)pk; (void)prec;
+    (void)pk;
     return c;
 }
 
