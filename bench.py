@@ -599,7 +599,9 @@ def our_arm(args):
                                       "grid-slices x%d" % ws,
                        "l2": "inputs (%.1f GB of lines) larger than L2" % (line_bytes / 1e9),
                        "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]}},
-            "gpu_launches": args.steps,
+            # per step: prep_kernel (S(T), width, y per line), voigt_ws_kernel
+            # (region I) and core_kernel (Humlicek regions II-IV)
+            "gpu_launches": 3 * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": traffic,
@@ -608,6 +610,10 @@ def our_arm(args):
                                         "no FP32 figure",
                          "flop_per_eval": fpe, "region_fractions": frac,
                          "launch_ms": launch_ms,
+                         "timed": "one cross-section per step: prep_kernel + voigt_ws_kernel "
+                                  "(region I) + core_kernel (regions II-IV), CUDA events on "
+                                  "the launching stream; per-kernel shares in the ncu launch "
+                                  "list under profiles/",
                          "line_stream_gbs": line_bytes / (launch_ms * 1e-3) / 1e9},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "path": "gexs_manager_* C ABI, pinned host",

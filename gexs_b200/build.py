@@ -19,6 +19,10 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
           "-I" + os.path.join(ROOT, "include")]
 SOURCES = [
     "csrc/gexs_kernels.cu",
+    "csrc/gexs_tiles_voigt.cu",
+    "csrc/gexs_tiles_erf.cu",
+    "csrc/gexs_tiles_gh16.cu",
+    "csrc/gexs_tiles_gh32.cu",
     "csrc/gexs_capi.cu",
     "csrc/gexs_calib.cu",
     "csrc/gexs_noalloc.cu",

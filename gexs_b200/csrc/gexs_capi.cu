@@ -89,9 +89,11 @@ static gexs_launch_cfg default_cfg(int pk, int prec)
     return c;
 }
 
-static bool cfg_ok(const gexs_launch_cfg& c)
+static bool cfg_ok(const gexs_launch_cfg& c, int prec)
 {
-    return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8) &&
+    /* 16 bins per lane only for the FP32 form */
+    return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8 ||
+            (c.bins_per_lane == 16 && prec == GEXS_FP32)) &&
            (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0;
 }
 
@@ -127,7 +129,7 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
             Group g; g.pk = pk; g.prec = prec; g.prefix.push_back(0);
             groups.push_back(g);
             gexs_launch_cfg c = cfg_in ? *cfg_in : ctx_cfg(ctx, pk, prec);
-            if (!cfg_ok(c)) return set_error(GEXS_ERR_INVALID, "launch configuration");
+            if (!cfg_ok(c, prec)) return set_error(GEXS_ERR_INVALID, "launch configuration");
             cfgs.push_back(c);
         }
         Group& g = groups[gi[key]];
@@ -506,7 +508,8 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
             return set_error(GEXS_ERR_INVALID, "autotune needs jobs of one profile and precision");
     std::vector<gexs_job> tj(jobs, jobs + njobs);
     for (auto& j : tj) j.accumulate = 0;          /* tuning runs overwrite outputs */
-    const int bins[3] = {2, 4, 8}, warps[2] = {4, 8};
+    const int bins[4] = {2, 4, 8, 16}, warps[2] = {4, 8};
+    const int nbins = (prec == GEXS_FP32) ? 4 : 3;
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
         return set_error(GEXS_ERR_CUDA, "stream");
@@ -514,7 +517,7 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     float best_ms = 1e30f; gexs_launch_cfg bc = default_cfg(pk, prec);
     int st = GEXS_OK;
-    for (int bi = 0; bi < 3 && !st; ++bi)
+    for (int bi = 0; bi < nbins && !st; ++bi)
         for (int wi = 0; wi < 2 && !st; ++wi) {
             gexs_launch_cfg c; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
             c.ctas_per_sm = 0; c.flags = 0;

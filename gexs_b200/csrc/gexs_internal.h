@@ -7,11 +7,13 @@
 
 namespace gexs {
 
-/* kernel launchers (gexs_kernels.cu) */
+/* kernel launchers (gexs_kernels.cu; tile kernels in gexs_tiles.cuh) */
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
 /* d_prep: device array of per-job prep arrays (S | invw | y, 3 N doubles
- * each, from launch_prep), or NULL to derive every line on load */
+ * each, from launch_prep), or NULL to derive every line on load.
+ * d_counter: a 256-byte block of work counters; the caller zeroes the
+ * first int, the FP32 Voigt core kernel's counter (int 32) is zeroed here. */
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,

@@ -150,7 +150,7 @@ int gexs_job_init(gexs_job* job, int convention, int profile,
 typedef struct gexs_ctx gexs_ctx;
 
 typedef struct gexs_launch_cfg {
-    int32_t bins_per_lane;   /* 2, 4 or 8                            */
+    int32_t bins_per_lane;   /* 2, 4 or 8; 16 for the FP32 form only */
     int32_t warps;           /* 4 or 8 (tile = 32*bins*warps)        */
     int32_t ctas_per_sm;     /* resident CTAs per SM (0 = max)       */
     int32_t flags;           /* GEXS_LAUNCH_*                        */
@@ -209,8 +209,9 @@ int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg
 
 /* ------------------------------------------------------ batched launches
  * A batch owns its device job table and work-item table; launching it is
- * one memset of the work counter plus one persistent kernel, which can be
- * captured once into a CUDA graph and replayed. */
+ * a memset of the work counter plus one persistent kernel per group of
+ * jobs (FP32 Voigt groups: a second memset and the core kernel), which can
+ * be captured once into a CUDA graph and replayed. */
 typedef struct gexs_batch gexs_batch;
 
 int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
