@@ -85,17 +85,6 @@ struct __align__(16) RecV {
                               lane's bins k = 0, 1 after adding wb + lane    */
 };
 
-/* a line whose core (Humlicek regions II-IV) reaches a sub-tile, for the
- * FP32 Voigt core kernel (64 bytes) */
-struct CoreRec {
-    double nu, invw, y;
-    double amp;            /* S * invw * out_scale                          */
-    int   rg[5];           /* single-region bin ranges a | b << 16: II, II,
-                              III, IV, IV (see core_ranges)                 */
-    float icf, fc, dx;     /* floor(tc), tc - floor(tc), dnu * invw         */
-    float yf, ampf;        /* FP32 copies of y and amp for region II        */
-    int   pad;
-};
 
 /* record type of a (profile class, precision) */
 template <int PK, int PREC> struct RecOf;
@@ -1159,103 +1148,56 @@ voigt_ws_kernel(const KArgs args)
 
 /* ------------------------------------------------- FP32 Voigt core kernel
  * The core of a line (its bins outside Humlicek region I: regions II, III,
- * IV) is evaluated here, after the tile kernel, and added into the output.
- * Kept out of the tile kernel so that kernel carries no FP64 Humlicek code
- * and no per-warp core rows (its registers and shared memory set how many
- * warps hide the MUFU and FMA latencies of the region-I loop).
+ * IV) is evaluated here, after the region-I kernel, and added into the
+ * output.  Kept out of that kernel so it carries no FP64 Humlicek code and
+ * no core accumulator rows.
  *
- * Work items are the tile kernel's tiles, each taken in sub-tiles of at
- * most CORE_W bins.  Per sub-tile: the lines whose core can reach it
+ * Work items are the region-I kernel's tiles, each taken in sub-tiles of at
+ * most CORE_W bins.  Per sub-tile, the lines whose core can reach it
  * (|f - nu| < 15 / invw = 15 nu dop_coef, inside the cutoff) are found by
- * two warp searches, derived 128 at a time with the tile kernel's FP64
- * predicates, and those with a core are compacted in line order.  Three
- * sweeps (region II in FP32, III and IV in FP64) deal the lines to warps
- * round-robin; in a sweep, lane l of a warp walks its own bins
- * t = l (mod 32) through the warp's lines, so lanes stay busy when cores
- * are narrow, no two lanes touch one bin, and each warp adds into its own
- * row of doubles.  Every bin thus receives its core terms in a fixed order
- * (region, then line), and the rows are added to the output in warp order:
- * results are bitwise independent of batching. */
+ * two warp searches and taken 32 at a time by the warps in turn, one line
+ * per lane, derived in FP64 with the region-I kernel's predicates.  A warp
+ * then steps through the union of its 32 lines' cores bin by bin: at bin t
+ * every lane evaluates its own line in the region t falls in (II in FP32,
+ * III and IV in FP64), a butterfly of shuffles sums the 32 terms in a fixed
+ * order, and lane 0 adds the sum into the warp's row of doubles.  Lines that
+ * are neighbours in nu have overlapping cores, so most lanes work at every
+ * step and no lane scans for work.  A bin receives its core terms in a
+ * fixed order (groups of 32 lines in ascending order per warp, rows added
+ * in warp order), so results are bitwise independent of batching. */
 constexpr int CORE_W = 1024;
 constexpr int CORE_WARPS = 4;
 
 struct CoreSmem {
     static constexpr int NT = CORE_WARPS * 32;
-    static constexpr size_t off_rows = 0;                                   /* WARPS x CORE_W doubles */
-    static constexpr size_t off_rec = off_rows + (size_t)CORE_WARPS * CORE_W * sizeof(double);
-    static constexpr size_t bytes = off_rec + (size_t)NT * sizeof(CoreRec);
+    static constexpr size_t bytes = (size_t)CORE_WARPS * CORE_W * sizeof(double);
 };
 
 /* the core of a line as single-region bin ranges, c3 within c2 within c1
  * (an empty inner range collapses to a point):
  * II = [c1a, c2a) u [c2b, c1b), III = [c3a, c3b), IV = [c2a, c3a) u [c3b, c2b) */
-__device__ __forceinline__ void core_ranges(int c1, int c2, int c3, int (&rg)[5])
+__device__ __forceinline__ void core_ranges(int c1, int c2, int c3, int& c1a, int& c1b,
+                                            int& c2a, int& c2b, int& c3a, int& c3b)
 {
-    const int c1a = lo16(c1), c1b = hi16(c1);
-    int c2a = lo16(c2), c2b = hi16(c2);
+    c1a = lo16(c1); c1b = hi16(c1);
+    c2a = lo16(c2); c2b = hi16(c2);
     if (c2a >= c2b) c2a = c2b = c1b;
-    int c3a = lo16(c3), c3b = hi16(c3);
+    c3a = lo16(c3); c3b = hi16(c3);
     if (c3a >= c3b) c3a = c3b = c2b;
-    rg[0] = pack2(c1a, c2a); rg[1] = pack2(c2b, c1b);
-    rg[2] = pack2(c3a, c3b);
-    rg[3] = pack2(c2a, c3a); rg[4] = pack2(c3b, c2b);
-}
-
-/* one sweep over region class R (2, 3, 4) */
-template <int R>
-__device__ __forceinline__ void core_sweep(const CoreRec* __restrict__ rec, int ncore, int warp,
-                                           int lane, double* __restrict__ row, double nu_start,
-                                           double dnu, int64_t j0)
-{
-    constexpr int S0 = (R == 2) ? 0 : (R == 3 ? 2 : 3);     /* first range slot */
-    constexpr int NSEG = (R == 3) ? 1 : 2;
-    int li = warp, seg = 0, cur = 0, t = 0, te = 0;
-    /* the next (line, range) of this warp holding a bin = lane (mod 32) */
-    auto next = [&]() -> bool {
-        while (li < ncore) {
-            const int r = rec[li].rg[S0 + seg];
-            const int a = lo16(r);
-            t = a + ((lane - a) & 31);
-            te = hi16(r);
-            cur = li;
-            if (++seg == NSEG) { seg = 0; li += CORE_WARPS; }
-            if (t < te) return true;
-        }
-        return false;
-    };
-    bool act = next();
-    while (__any_sync(0xffffffffu, act)) {
-        if (act) {
-            const CoreRec& q = rec[cur];
-            double v;
-            if constexpr (R == 2) {
-                const float x = fabsf(((float)t - q.icf) - q.fc) * q.dx;
-                v = (double)(q.ampf * hum_region2<float>(x, q.yf));
-            } else {
-                const double x = dmul(fabs(dsub(grid_f(nu_start, dnu, j0 + t), q.nu)), q.invw);
-                v = q.amp * (R == 3 ? hum_region3<double>(x, q.y) : hum_region4<double>(x, q.y));
-            }
-            row[t] += v;
-            t += 32;
-            if (t >= te) act = next();
-        }
-    }
 }
 
 template <bool PREP>
 __global__ void __launch_bounds__(CORE_WARPS * 32)
 core_kernel(const KArgs args)
 {
-    typedef CoreSmem L;
-    constexpr int NT = L::NT;
+    constexpr int NT = CoreSmem::NT;
     extern __shared__ __align__(16) unsigned char smem[];
-    double*  s_rows = reinterpret_cast<double*>(smem + L::off_rows);
-    CoreRec* s_rec = reinterpret_cast<CoreRec*>(smem + L::off_rec);
+    double* s_rows = reinterpret_cast<double*>(smem);
     __shared__ int s_item;
     __shared__ long long s_lohi[2];
-    __shared__ int s_wcount[CORE_WARPS];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* row = s_rows + warp * CORE_W;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(args.counter, 1);
         __syncthreads();
@@ -1265,7 +1207,7 @@ core_kernel(const KArgs args)
         while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= item) jl = m; else jh = m; }
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
-        /* the tile kernel's tile width for this launch */
+        /* the region-I kernel's tile of this item */
         const int64_t t0 = J.start_idx + (int64_t)(item - __ldg(args.prefix + jl)) * args.tile_w;
         const int64_t tend = min((int64_t)(t0 + args.tile_w), J.start_idx + J.n_points);
         const int64_t nl = J.lines.count;
@@ -1295,15 +1237,17 @@ core_kernel(const KArgs args)
             for (int z = tid; z < CORE_WARPS * CORE_W; z += NT) s_rows[z] = 0.0;
             __syncthreads();
             const int64_t lo = s_lohi[0], hi = max((int64_t)s_lohi[1], lo);
-            for (int64_t base = lo; base < hi; base += NT) {
-                const int64_t i = base + tid;
+            for (int64_t g0 = lo + (int64_t)warp * 32; g0 < hi; g0 += NT) {
+                const int64_t i = g0 + lane;
                 bool has = false;
-                CoreRec cr;
+                int c1a = 0, c1b = 0, c2a = 0, c2b = 0, c3a = 0, c3b = 0;
+                double nu = 0.0, invw = 0.0, y = 0.0, amp = 0.0;
+                float icf = 0.f, fc = 0.f, dx = 0.f, yf = 0.f, ampf = 0.f;
                 if (i < hi) {
                     LineQ lq;
                     if constexpr (PREP) {
-                        const double nu = __ldg(J.lines.nu + i);
-                        lq.nu = nu == 0.0 ? 1e-6 : nu;
+                        const double v = __ldg(J.lines.nu + i);
+                        lq.nu = v == 0.0 ? 1e-6 : v;
                         lq.S = __ldg(pb + i); lq.invw = __ldg(pb + nl + i); lq.y = __ldg(pb + 2 * nl + i);
                     } else {
                         RawLine Lr;
@@ -1315,38 +1259,42 @@ core_kernel(const KArgs args)
                     Derived<PK_VOIGT> d = derive_line<PK_VOIGT>(T, lq, 10.5);
                     if (lo16(d.c1) < hi16(d.c1)) {
                         has = true;
+                        core_ranges(d.c1, d.c2, d.c3, c1a, c1b, c2a, c2b, c3a, c3b);
                         const double ic = fmin(fmax(floor(d.tc), -8388608.0), 8388607.0);
-                        cr.nu = d.nu; cr.invw = d.invw; cr.y = d.y;
-                        cr.amp = dmul(dmul(d.S, d.invw), J.out_scale);
-                        core_ranges(d.c1, d.c2, d.c3, cr.rg);
-                        cr.pad = 0;
-                        cr.icf = (float)ic; cr.fc = (float)(d.tc - ic);
-                        cr.dx = (float)dmul(J.dnu, d.invw);
-                        cr.yf = (float)d.y; cr.ampf = (float)cr.amp;
+                        nu = d.nu; invw = d.invw; y = d.y;
+                        amp = dmul(dmul(d.S, d.invw), J.out_scale);
+                        icf = (float)ic; fc = (float)(d.tc - ic);
+                        dx = (float)dmul(J.dnu, d.invw);
+                        yf = (float)y; ampf = (float)amp;
                     }
                 }
-                /* compaction in line order */
-                const unsigned bal = __ballot_sync(0xffffffffu, has);
-                if (lane == 0) s_wcount[warp] = __popc(bal);
-                __syncthreads();
-                int off = 0, ncore = 0;
+                /* union of the warp's cores */
+                int ulo = has ? c1a : INT32_MAX, uhi = has ? c1b : INT32_MIN;
 #pragma unroll
-                for (int w = 0; w < CORE_WARPS; ++w) {
-                    const int cw = s_wcount[w];
-                    if (w < warp) off += cw;
-                    ncore += cw;
+                for (int o = 16; o > 0; o >>= 1) {
+                    ulo = min(ulo, __shfl_xor_sync(0xffffffffu, ulo, o));
+                    uhi = max(uhi, __shfl_xor_sync(0xffffffffu, uhi, o));
                 }
-                if (has) s_rec[off + __popc(bal & ((1u << lane) - 1u))] = cr;
-                __syncthreads();
-                if (ncore) {
-                    double* row = s_rows + warp * CORE_W;
-                    core_sweep<2>(s_rec, ncore, warp, lane, row, J.nu_start, J.dnu, T.j0);
-                    core_sweep<3>(s_rec, ncore, warp, lane, row, J.nu_start, J.dnu, T.j0);
-                    core_sweep<4>(s_rec, ncore, warp, lane, row, J.nu_start, J.dnu, T.j0);
+                for (int t = ulo; t < uhi; ++t) {
+                    double v = 0.0;
+                    if (has && t >= c1a && t < c1b) {
+                        if (t < c2a || t >= c2b) {
+                            const float x = fabsf(((float)t - icf) - fc) * dx;
+                            v = (double)(ampf * hum_region2<float>(x, yf));
+                        } else {
+                            const double x = dmul(fabs(dsub(grid_f(J.nu_start, J.dnu, T.j0 + t), nu)), invw);
+                            v = amp * ((t >= c3a && t < c3b) ? hum_region3<double>(x, y)
+                                                             : hum_region4<double>(x, y));
+                        }
+                    }
+                    /* fixed-order sum of the 32 lines' terms; lane 0's value is used */
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0) row[t] += v;
                 }
-                __syncthreads();
             }
-            /* rows in warp order, added to the tile kernel's result */
+            __syncthreads();
+            /* rows in warp order, added to the region-I result */
             for (int t = tid; t < T.jn; t += NT) {
                 double v = 0.0;
                 bool any = false;
