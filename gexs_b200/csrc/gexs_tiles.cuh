@@ -142,6 +142,9 @@ struct Tile {
     int64_t j0;          /* absolute first bin                       */
     int     jn;          /* bins in this tile                        */
     double  f0, fl;      /* frequencies of first / last bin          */
+    double  inv_dnu;     /* 1 / dnu: tile-relative centres (search
+                            guesses and FP32 offsets; every window and
+                            region decision uses exact predicates)   */
 };
 
 /* window of a line inside the tile as [a, b) (tile-relative) */
@@ -248,15 +251,17 @@ __device__ __forceinline__ LineQ line_quantities(const gexs_job& J, const RawLin
     return q;
 }
 
-/* tile-dependent part: centre in bins, window and Humlicek region limits */
+/* tile-dependent part: centre in bins, window and Humlicek region limits
+ * (inlined into the warp-specialised producers; derive_line below is the
+ * out-of-line form for kernels that interleave it with their FP32 loops) */
 template <int PK>
-__device__ __noinline__ Derived<PK> derive_line(const Tile& T, const LineQ& q, double zthr)
+__device__ __forceinline__ Derived<PK> derive_line_body(const Tile& T, const LineQ& q, double zthr)
 {
     const gexs_job& J = *T.J;
     Derived<PK> d;
     const double nu = q.nu;
     d.nu = nu; d.S = q.S; d.invw = q.invw; d.y = q.y;
-    d.tc = ddiv(dsub(nu, T.f0), J.dnu);
+    d.tc = dmul(dsub(nu, T.f0), T.inv_dnu);
     int a, b;
     tile_window(T, nu, d.tc, &a, &b);
     d.win = pack2(a, b);
@@ -287,6 +292,12 @@ __device__ __noinline__ Derived<PK> derive_line(const Tile& T, const LineQ& q, d
                         });
     }
     return d;
+}
+
+template <int PK>
+__device__ __noinline__ Derived<PK> derive_line(const Tile& T, const LineQ& q, double zthr)
+{
+    return derive_line_body<PK>(T, q, zthr);
 }
 
 /* ------------------------------------------------------------ kernel args */
@@ -739,6 +750,7 @@ tile_kernel(const KArgs args)
         T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
         T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
         T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
+        T.inv_dnu = 1.0 / J.dnu;
 
         const int64_t nl = J.lines.count;
         const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
@@ -1013,6 +1025,7 @@ voigt_ws_kernel(const KArgs args)
             T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
             T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
             T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
+            T.inv_dnu = 1.0 / J.dnu;
             const int64_t nl = J.lines.count;
             const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
             if (pw == 0) {
@@ -1076,7 +1089,7 @@ voigt_ws_kernel(const KArgs args)
                             Lr.g = s_gn[o]; Lr.gam = s_f[6 * NP + o]; Lr.nexp = s_f[8 * NP + o];
                             lq = line_quantities<true>(J, Lr);
                         }
-                        Derived<PK_VOIGT> d = derive_line<PK_VOIGT>(T, lq, 10.5);
+                        Derived<PK_VOIGT> d = derive_line_body<PK_VOIGT>(T, lq, 10.5);
                         RecV rr;
                         make_rec<PK_VOIGT, B, CONS>(rr, d, J, T);
                         rec[r] = rr;
@@ -1220,6 +1233,7 @@ core_kernel(const KArgs args)
             T.jn = (int)min((int64_t)CORE_W, tend - s0);
             T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
             T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
+            T.inv_dnu = 1.0 / J.dnu;
             const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
             /* a core reaches f only if |f - nu| < 15 nu dop_coef */
             double vlo = T.f0 - J.cutoff, vhi = T.fl + J.cutoff;
