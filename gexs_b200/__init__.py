@@ -8,4 +8,5 @@ view used by tests and the benchmark.
 from ._capi import (GAUSSIAN, DOPPLER, VOIGT, VOIGT_QUAD, FP64, FP32,  # noqa: F401
                     WINDOW_INCLUSIVE, WINDOW_ROUNDED, ERF_STABLE, ERF_LITERAL,
                     CONV_PHYSICAL, CONV_REF_CPU, CONV_REF_GPU, GexsError, LIB_PATH)
-from .engine import Context, Job, LineList, Manager, Batch, Server, job_init  # noqa: F401
+from .engine import (Context, Job, LineList, Manager, Batch, Server, job_init,  # noqa: F401
+                     parse_exomol, load_exomol)

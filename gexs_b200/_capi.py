@@ -64,6 +64,20 @@ class GexsRequestInfo(C.Structure):
                 ("status", C.c_int32)]
 
 
+BROAD_DEFAULTS, BROAD_BY_J = 0, 1
+
+
+class GexsStateTable(C.Structure):
+    _fields_ = [("energy", C.c_void_p), ("g", C.c_void_p), ("J", C.c_void_p),
+                ("count", C.c_int64)]
+
+
+class GexsLineTable(C.Structure):
+    _fields_ = [("nu", C.c_void_p), ("elow", C.c_void_p), ("aif", C.c_void_p),
+                ("gns", C.c_void_p), ("gamma", C.c_void_p), ("n", C.c_void_p),
+                ("count", C.c_int64)]
+
+
 # (name, restype, argtypes) for every symbol of include/gexs_b200.h and
 # include/gexs_serve.h
 SIGNATURES = [
@@ -93,6 +107,18 @@ SIGNATURES = [
     ("gexs_partition", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
     ("gexs_probe_fp32_tflops", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    ("gexs_exomol_parse_states", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64,
+                                           C.POINTER(GexsStateTable)]),
+    ("gexs_exomol_parse_trans", C.c_int, [C.c_void_p, C.POINTER(GexsStateTable), C.c_char_p,
+                                          C.c_int64, C.c_char_p, C.c_int64, C.c_int, C.c_double,
+                                          C.c_double, C.c_int, C.POINTER(GexsLineTable)]),
+    ("gexs_exomol_load", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                   C.c_double, C.c_double, C.c_int, C.POINTER(GexsStateTable),
+                                   C.POINTER(GexsLineTable)]),
+    ("gexs_state_table_export", C.c_int, [C.POINTER(GexsStateTable)] + [C.c_void_p] * 3),
+    ("gexs_line_table_export", C.c_int, [C.POINTER(GexsLineTable)] + [C.c_void_p] * 6),
+    ("gexs_state_table_free", C.c_int, [C.POINTER(GexsStateTable)]),
+    ("gexs_line_table_free", C.c_int, [C.POINTER(GexsLineTable)]),
     ("gexs_manager_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
                                       C.POINTER(C.c_void_p)]),
     ("gexs_manager_destroy", C.c_int, [C.c_void_p]),

@@ -26,6 +26,7 @@ SOURCES = [
     "csrc/gexs_capi.cu",
     "csrc/gexs_calib.cu",
     "csrc/gexs_noalloc.cu",
+    "csrc/gexs_ingest.cu",
     "host/B200Manager.cpp",
     "host/gexs_server.cpp",
 ]

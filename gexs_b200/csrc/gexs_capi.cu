@@ -75,6 +75,11 @@ struct gexs_ctx {
     std::map<int, gexs_launch_cfg> tuned;   /* key: pk*4 + prec */
 };
 
+namespace gexs {
+int ctx_device(gexs_ctx* c) { return c->device; }
+int ctx_sm_count(gexs_ctx* c) { return c->nsm; }
+}  // namespace gexs
+
 static gexs_launch_cfg default_cfg(int pk, int prec)
 {
     /* measured best on B200 for the 1e8-line Voigt workload (FP32: 4 bins x

@@ -26,6 +26,10 @@ cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,
                              const double* d_betas, int nt, double* d_partial, int nchunk,
                              double* d_q, cudaStream_t st);
 
+/* context accessors (gexs_capi.cu) */
+int ctx_device(gexs_ctx* c);
+int ctx_sm_count(gexs_ctx* c);
+
 /* error reporting (gexs_capi.cu): thread-local message, returns status */
 int set_error(int status, const std::string& msg);
 int cuda_error(cudaError_t e, const char* where);

@@ -191,6 +191,62 @@ class Context:
         return q
 
 
+# ---------------------------------------------------------------- ingest
+def _export_states(t, device):
+    import torch
+    n = int(t.count)
+    e = torch.empty(n, dtype=torch.float64, device=device)
+    g = torch.empty(n, dtype=torch.int32, device=device)
+    j = torch.empty(n, dtype=torch.int32, device=device)
+    if n:
+        check(lib().gexs_state_table_export(C.byref(t), _ptr(e), _ptr(g), _ptr(j)),
+              "gexs_state_table_export")
+    lib().gexs_state_table_free(C.byref(t))
+    return {"energy": e, "g": g, "J": j}
+
+
+def _export_lines(t, device):
+    import torch
+    n = int(t.count)
+    d = {k: torch.empty(n, dtype=torch.float64, device=device)
+         for k in ("nu", "elow", "aif", "gamma", "n")}
+    d["gns"] = torch.empty(n, dtype=torch.int32, device=device)
+    if n:
+        check(lib().gexs_line_table_export(C.byref(t), _ptr(d["nu"]), _ptr(d["elow"]),
+                                           _ptr(d["aif"]), _ptr(d["gns"]), _ptr(d["gamma"]),
+                                           _ptr(d["n"])), "gexs_line_table_export")
+    lib().gexs_line_table_free(C.byref(t))
+    return d
+
+
+def parse_exomol(ctx, states_text, trans_text, broad_text=b"", broad_mode=capi.BROAD_DEFAULTS,
+                 default_gamma=0.1, default_n=0.1, sort_by_nu=True, device="cuda"):
+    """ExoMol .states/.trans (and .broad) text parsed on the GPU (gexs_exomol_*):
+    returns (states dict, lines dict) of torch device tensors."""
+    st = capi.GexsStateTable()
+    check(lib().gexs_exomol_parse_states(ctx.h, states_text, len(states_text), C.byref(st)),
+          "gexs_exomol_parse_states")
+    lt = capi.GexsLineTable()
+    rc = lib().gexs_exomol_parse_trans(ctx.h, C.byref(st), trans_text, len(trans_text),
+                                       broad_text, len(broad_text), broad_mode, default_gamma,
+                                       default_n, 1 if sort_by_nu else 0, C.byref(lt))
+    if rc != capi.GEXS_OK:
+        lib().gexs_state_table_free(C.byref(st))
+        check(rc, "gexs_exomol_parse_trans")
+    return _export_states(st, device), _export_lines(lt, device)
+
+
+def load_exomol(ctx, states_path, trans_path, broad_path=None, broad_mode=capi.BROAD_DEFAULTS,
+                default_gamma=0.1, default_n=0.1, sort_by_nu=True, device="cuda"):
+    """gexs_exomol_load: read the files on the host, parse on the GPU."""
+    st, lt = capi.GexsStateTable(), capi.GexsLineTable()
+    check(lib().gexs_exomol_load(ctx.h, states_path.encode(), trans_path.encode(),
+                                 broad_path.encode() if broad_path else None, broad_mode,
+                                 default_gamma, default_n, 1 if sort_by_nu else 0,
+                                 C.byref(st), C.byref(lt)), "gexs_exomol_load")
+    return _export_states(st, device), _export_lines(lt, device)
+
+
 class Manager:
     """The drop-in BaseManager (B200Manager) through its flat C wrappers;
     host numpy arrays in and out, exactly as BaseProfile passes them."""

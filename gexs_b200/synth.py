@@ -120,3 +120,111 @@ def make_lines_torch(states, ntrans, nu_min, nu_max, seed, broadening_seed=None,
         out["gamma"] = torch.empty(m, device=device, dtype=torch.float64).uniform_(0.03, 0.1, generator=g2)
         out["n"] = torch.empty(m, device=device, dtype=torch.float64).uniform_(0.4, 0.8, generator=g2)
     return out
+
+
+# ------------------------------------------------------------------ ExoMol text
+# Fixed-width text in the layout of ExoMol files, formatted with numpy
+# (vectorised: 1e7-line files in seconds).  The text itself is the ground
+# truth of the ingest tests: the parsers are compared on the bytes.
+def _digits(v, width, pad=b" "):
+    """Right-aligned decimal of non-negative int64 v in `width` columns."""
+    v = np.asarray(v, dtype=np.int64)
+    out = np.full((v.shape[0], width), pad[0], dtype=np.uint8)
+    rem = v.copy()
+    for k in range(width - 1, -1, -1):
+        d = (rem % 10).astype(np.uint8)
+        nz = (rem > 0) | (k == width - 1)
+        out[:, k] = np.where(nz, d + ord("0"), out[:, k])
+        rem //= 10
+    return out
+
+
+def _zeros(v, width):
+    """Zero-padded decimal of non-negative int64 v in `width` columns."""
+    v = np.asarray(v, dtype=np.int64)
+    out = np.empty((v.shape[0], width), dtype=np.uint8)
+    rem = v.copy()
+    for k in range(width - 1, -1, -1):
+        out[:, k] = (rem % 10).astype(np.uint8) + ord("0")
+        rem //= 10
+    return out
+
+
+def _col(n, ch):
+    return np.full((n, 1), ord(ch), dtype=np.uint8)
+
+
+def _fixed(x, width, prec):
+    """Non-negative x as '%{width}.{prec}f'-like text (rounded half up)."""
+    scale = 10 ** prec
+    v = np.floor(np.asarray(x, dtype=np.float64) * scale + 0.5).astype(np.int64)
+    return np.hstack([_digits(v // scale, width - prec - 1), _col(len(v), "."),
+                      _zeros(v % scale, prec)])
+
+
+def _sci(x, mant=4):
+    """Positive x as 'd.ddddE+XX'."""
+    x = np.asarray(x, dtype=np.float64)
+    e = np.floor(np.log10(x)).astype(np.int64)
+    m = np.floor(x / np.power(10.0, e) * 10 ** mant + 0.5).astype(np.int64)
+    over = m >= 10 ** (mant + 1)
+    m = np.where(over, m // 10, m)
+    e = np.where(over, e + 1, e)
+    under = m < 10 ** mant
+    m = np.where(under, m * 10, m)
+    e = np.where(under, e - 1, e)
+    n = len(x)
+    sign = np.where(e < 0, ord("-"), ord("+")).astype(np.uint8)[:, None]
+    return np.hstack([_zeros(m // 10 ** mant, 1), _col(n, "."), _zeros(m % 10 ** mant, mant),
+                      _col(n, "E"), sign, _zeros(np.abs(e), 2)])
+
+
+def exomol_states_text(states):
+    """`id E g J` lines (ids 1..N in order), as ExoMol .states files."""
+    n = len(states.energy)
+    rows = np.hstack([_digits(np.arange(1, n + 1), 12), _col(n, " "),
+                      _fixed(states.energy, 12, 6), _col(n, " "), _digits(states.g, 6),
+                      _col(n, " "), _digits(states.j, 7), _col(n, "\n")])
+    return rows.tobytes()
+
+
+def exomol_trans_text(upper, lower, aif, nu=None):
+    """`id_upper id_lower A [nu]` lines (1-based ids), as ExoMol .trans files."""
+    n = len(upper)
+    parts = [_digits(np.asarray(upper) + 1, 12), _col(n, " "), _digits(np.asarray(lower) + 1, 12),
+             _col(n, " "), _sci(aif)]
+    if nu is not None:
+        parts += [_col(n, " "), _fixed(nu, 12, 6)]
+    parts.append(_col(n, "\n"))
+    return np.hstack(parts).tobytes()
+
+
+def exomol_broad_text(j_max, seed, a1_pairs=0):
+    """`a0 gamma n J''` lines for J'' = 0..j_max (and some `a1 gamma n J'' J'`)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for j in range(j_max + 1):
+        out.append("a0 %.4f %.3f %d" % (rng.uniform(0.03, 0.1), rng.uniform(0.4, 0.8), j))
+    for _ in range(a1_pairs):
+        j = int(rng.integers(0, j_max + 1))
+        out.append("a1 %.4f %.3f %d %d" % (rng.uniform(0.03, 0.1), rng.uniform(0.4, 0.8), j,
+                                           j + int(rng.integers(-1, 2))))
+    return ("\n".join(out) + "\n").encode()
+
+
+def make_exomol_transitions(states, ntrans, nu_min, nu_max, seed):
+    """Upper/lower indices (0-based) and A of seeded transitions, file order
+    (not sorted by nu)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    order = np.argsort(states.energy, kind="stable")
+    es = states.energy[order]
+    lower = rng.integers(0, len(es), ntrans)
+    le = es[lower]
+    lo = np.searchsorted(es, le + nu_min, side="left")
+    hi = np.searchsorted(es, le + nu_max, side="right")
+    ok = hi > lo
+    lower, lo, hi = lower[ok], lo[ok], hi[ok]
+    up = lo + np.floor(rng.random(len(lower)) * (hi - lo)).astype(np.int64)
+    up = np.minimum(up, hi - 1)
+    aif = 10.0 ** rng.uniform(-6.0, 2.0, len(lower))
+    return order[up].astype(np.int64), order[lower].astype(np.int64), aif

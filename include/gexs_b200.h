@@ -207,6 +207,65 @@ int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
 int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
                      void* stream);
 
+/* --------------------------------------------------------- ExoMol ingest
+ * The reader layer of the reference (Readers/Exomol/ExomolStateReader.cpp,
+ * Readers/Exomol/exomol_functions.cpp) on the GPU: text is copied to the
+ * device once and parsed there, one thread per record, with the
+ * reference's number semantics (see gexs_ingest.cu); results are device
+ * tables owned by the caller (free with the *_free functions).
+ *  - states: one per text line, in line order (exomol_functions.cpp:8-48:
+ *    id/gns/J by strtol base 0, energy by strtod; index = line number);
+ *    a line longer than 1022 bytes is an error (the reference's fgets
+ *    buffer would split it).
+ *  - transitions: per non-empty line `id_upper id_lower A [more fields]`
+ *    (ExomolStateReader.cpp:132-172): nu = E_u - E_l, elow = E_l,
+ *    gns = g_u; ids must lie in [1, states->count].
+ *  - broadening: GEXS_BROAD_DEFAULTS gives every line default_gamma and
+ *    default_n, which is what the reference's lookup yields
+ *    (ExomolStateReader.cpp:21 keeps the failed key, no entry matches);
+ *    GEXS_BROAD_BY_J uses "a1 gamma n J'' J'" entries, then "a0 gamma n J''",
+ *    then the defaults.  A missing broadener file means defaults.
+ *  - sort_by_nu != 0: lines sorted by nu (stable), as the cross-section
+ *    path requires; 0 keeps file order. */
+#define GEXS_BROAD_DEFAULTS 0
+#define GEXS_BROAD_BY_J     1
+
+typedef struct gexs_state_table {
+    double*  energy;   /* device, cm^-1 */
+    int32_t* g;        /* device, total degeneracy */
+    int32_t* J;        /* device */
+    int64_t  count;
+} gexs_state_table;
+
+typedef struct gexs_line_table {   /* device arrays, same meaning as gexs_lines */
+    double*  nu;
+    double*  elow;
+    double*  aif;
+    int32_t* gns;
+    double*  gamma;
+    double*  n;
+    int64_t  count;
+} gexs_line_table;
+
+int gexs_exomol_parse_states(gexs_ctx* ctx, const char* h_text, int64_t nbytes,
+                             gexs_state_table* out);
+int gexs_exomol_parse_trans(gexs_ctx* ctx, const gexs_state_table* states, const char* h_text,
+                            int64_t nbytes, const char* h_broad, int64_t broad_nbytes,
+                            int broad_mode, double default_gamma, double default_n,
+                            int sort_by_nu, gexs_line_table* out);
+/* read the files (broad_path may be NULL) and parse both */
+int gexs_exomol_load(gexs_ctx* ctx, const char* states_path, const char* trans_path,
+                     const char* broad_path, int broad_mode, double default_gamma,
+                     double default_n, int sort_by_nu, gexs_state_table* states_out,
+                     gexs_line_table* lines_out);
+/* copy a table into caller-owned device arrays of `count` elements */
+int gexs_state_table_export(const gexs_state_table* t, double* d_energy, int32_t* d_g,
+                            int32_t* d_J);
+int gexs_line_table_export(const gexs_line_table* t, double* d_nu, double* d_elow, double* d_aif,
+                           int32_t* d_gns, double* d_gamma, double* d_n);
+int gexs_state_table_free(gexs_state_table* t);
+int gexs_line_table_free(gexs_line_table* t);
+
 /* ------------------------------------------------------ batched launches
  * A batch owns its device job table and work-item table; launching it is
  * a memset of the work counter plus one persistent kernel per group of

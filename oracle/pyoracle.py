@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgexsref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libgexsref_fast.so")
+REF_READER_BIN = os.path.join(HERE, "_ref", "gexsref_reader")
 
 _orc = None
 _refs = {}
@@ -52,6 +53,16 @@ def orc():
         h.orc_region_hist.argtypes = [C.POINTER(GexsJob), C.POINTER(C.c_int64)]
         h.orc_line_params.restype = C.c_int
         h.orc_line_params.argtypes = [C.POINTER(GexsJob), C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_exomol_states.restype = C.c_int64
+        h.orc_exomol_states.argtypes = [C.c_char_p, C.c_int64] + [C.c_void_p] * 3 + [C.c_int64]
+        h.orc_exomol_trans.restype = C.c_int64
+        h.orc_exomol_trans.argtypes = ([C.c_char_p, C.c_int64] + [C.c_void_p] * 3 +
+                                       [C.c_int64, C.c_char_p, C.c_int64, C.c_int, C.c_double,
+                                        C.c_double] + [C.c_void_p] * 6 + [C.c_int64])
+        h.orc_sort_by_nu.restype = None
+        h.orc_sort_by_nu.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        h.orc_strtod.restype = C.c_double
+        h.orc_strtod.argtypes = [C.c_char_p]
         _orc = h
     return _orc
 
@@ -151,3 +162,62 @@ def ref_partition(energy, g, temp, fast=False):
 
 def ref_humlic(x, y):
     return ref().ref_humlic(x, y)
+
+
+# ------------------------------------------------------------------ ExoMol ingest
+def exomol_states(text):
+    """Restated exomol_functions.cpp:8-48: (energy, g, J) per fgets line."""
+    h = orc()
+    n = h.orc_exomol_states(text, len(text), None, None, None, 0)
+    e = np.zeros(n, np.float64); g = np.zeros(n, np.int32); j = np.zeros(n, np.int32)
+    h.orc_exomol_states(text, len(text), _p(e), _p(g), _p(j), n)
+    return e, g, j
+
+
+def exomol_trans(text, energy, g, j, broad=b"", mode=0, default_gamma=0.1, default_n=0.1,
+                 sort_by_nu=False):
+    """Restated ExomolStateReader.cpp:132-172 (token stream), file order or
+    stably sorted by nu."""
+    h = orc()
+    energy = np.ascontiguousarray(energy, np.float64)
+    g = np.ascontiguousarray(g, np.int32); j = np.ascontiguousarray(j, np.int32)
+    args = (text, len(text), _p(energy), _p(g), _p(j), len(energy), broad, len(broad), mode,
+            default_gamma, default_n)
+    n = h.orc_exomol_trans(*args, None, None, None, None, None, None, 0)
+    if n < 0:
+        raise ValueError("state id out of range")
+    d = {k: np.zeros(n, np.float64) for k in ("nu", "elow", "aif", "gamma", "n")}
+    d["gns"] = np.zeros(n, np.int32)
+    h.orc_exomol_trans(*args, _p(d["nu"]), _p(d["elow"]), _p(d["aif"]), _p(d["gns"]),
+                       _p(d["gamma"]), _p(d["n"]), n)
+    if sort_by_nu and n:
+        perm = np.zeros(n, np.int64)
+        h.orc_sort_by_nu(_p(d["nu"]), n, _p(perm))
+        d = {k: v[perm] for k, v in d.items()}
+    return d
+
+
+def strtod(s):
+    return orc().orc_strtod(s)
+
+
+def ref_reader_available():
+    return os.path.exists(REF_READER_BIN)
+
+
+def ref_exomol_read(states_path, trans_path, broad_path=None, default_gamma=0.1, default_n=0.1):
+    """The reference's ExomolStateReader (compiled from its sources, run as
+    oracle/_ref/gexsref_reader): every transition in file order as
+    (nu, gns, e_i, aif, gamma, n)."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "ref.bin")
+        subprocess.run([REF_READER_BIN, states_path, trans_path, broad_path or "-",
+                        repr(float(default_gamma)), repr(float(default_n)), out], check=True,
+                       stdout=subprocess.DEVNULL)
+        raw = np.fromfile(out, dtype=np.uint8)
+    n = int(raw[:8].view(np.int64)[0])
+    arr = raw[8:].view(np.float64).reshape(6, n) if n else np.zeros((6, 0))
+    keys = ("nu", "gns", "elow", "aif", "gamma", "n")
+    return {k: arr[i].copy() for i, k in enumerate(keys)}
