@@ -441,6 +441,59 @@ def quad_suite(args):
     return {"lines": lines.count, "grid_points": G, "temperature": T, "rows": res}
 
 
+def ingest_suite(args):
+    """ExoMol ingest: seeded .states (2e5 states, J 0-80) and .trans (the
+    --ingest-lines transitions, 30-7000 cm^-1) text in the ExoMol layout,
+    parsed on the GPU from host bytes (gexs_exomol_parse_states/trans: H2D
+    copy, newline index, parse, state lookup, stable nu sort), against the
+    reference's own ExomolStateReader (compiled from its sources) on a
+    bounded sample of the same file, single-threaded as in the reference."""
+    import subprocess
+    import tempfile
+    import torch
+    from gexs_b200 import Context, synth
+    from gexs_b200.engine import parse_exomol
+    from oracle import pyoracle as po
+    st = synth.make_states(200000, 80, 1006)
+    u, l, a = synth.make_exomol_transitions(st, args.ingest_lines, 30.0, 7000.0, 2006)
+    stext = synth.exomol_states_text(st)
+    ttext = synth.exomol_trans_text(u, l, a)
+    ctx = Context(0)
+    parse_exomol(ctx, stext, ttext[:1 << 20].rsplit(b"\n", 1)[0] + b"\n")   # warm-up
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S, L = parse_exomol(ctx, stext, ttext, sort_by_nu=True)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    n = int(L["nu"].numel())
+    best = min(times)
+    res = {"suite": "ingest", "transitions": n, "states": len(st.energy),
+           "text_bytes": len(ttext) + len(stext), "gpu_s": best,
+           "gpu_lines_per_s": n / best, "gpu_text_gbs": (len(ttext) + len(stext)) / best / 1e9,
+           "timed": "host bytes -> device text -> sorted device line table, wall clock with "
+                    "device syncs (includes the H2D copy of the text)"}
+    if po.ref_reader_available():
+        k = min(n, 2_000_000)
+        cut = ttext[:k * (len(ttext) // max(len(u), 1))]
+        cut = cut[:cut.rfind(b"\n") + 1]
+        with tempfile.TemporaryDirectory() as td:
+            sp, tp = os.path.join(td, "s.states"), os.path.join(td, "s.trans")
+            open(sp, "wb").write(stext)
+            open(tp, "wb").write(cut)
+            t0 = time.perf_counter()
+            subprocess.run([po.REF_READER_BIN, sp, tp, "-", "0.1", "0.1", os.path.join(td, "o")],
+                           check=True, stdout=subprocess.DEVNULL)
+            dt = time.perf_counter() - t0
+        nref = cut.count(b"\n")
+        res["reference_cpu"] = {"lines_per_s": nref / dt, "lines": nref, "s": dt, "threads": 1,
+                                "note": "states load + transition stream of the reference reader, "
+                                        "one process (the reference reads on one thread)"}
+        res["speedup_vs_reference"] = res["gpu_lines_per_s"] / res["reference_cpu"]["lines_per_s"]
+    return res
+
+
 def e2e_manager(torch, dev, L, q, steps, warmup, local_rank):
     """Same workload through the drop-in manager's C ABI with host buffers."""
     from gexs_b200 import _capi as capi
@@ -652,8 +705,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--suite", default="main", choices=["main", "quad"],
-                    help="quad: Gauss-Hermite 16/32 vs Humlicek on the 5e8-line list")
+    ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest"],
+                    help="quad: Gauss-Hermite 16/32 vs Humlicek on the 5e8-line list; "
+                         "ingest: ExoMol text parsed on the GPU vs the reference reader")
+    ap.add_argument("--ingest-lines", type=int, default=20_000_000)
     ap.add_argument("--quad-lines", type=int, default=500_000_000)
     ap.add_argument("--shard", default="replica", choices=["replica", "grid"],
                     help="N>1: one cross-section per rank (weak) or slices of one (strong)")
@@ -670,6 +725,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if args.suite == "ingest":
+        print(json.dumps(ingest_suite(args)), flush=True)
+        return 0
     if args.suite == "quad":
         r = quad_suite(args)
         print(json.dumps({"suite": "voigt-quad", "unit": UNIT, **r}), flush=True)

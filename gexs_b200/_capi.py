@@ -78,8 +78,8 @@ class GexsLineTable(C.Structure):
                 ("count", C.c_int64)]
 
 
-# (name, restype, argtypes) for every symbol of include/gexs_b200.h and
-# include/gexs_serve.h
+# (name, restype, argtypes) for every symbol of include/gexs_b200.h,
+# include/gexs_serve.h and include/gexs_reader.h
 SIGNATURES = [
     ("gexs_version", C.c_int, []),
     ("gexs_status_string", C.c_char_p, [C.c_int]),
@@ -118,6 +118,15 @@ SIGNATURES = [
     ("gexs_state_table_export", C.c_int, [C.POINTER(GexsStateTable)] + [C.c_void_p] * 3),
     ("gexs_line_table_export", C.c_int, [C.POINTER(GexsLineTable)] + [C.c_void_p] * 6),
     ("gexs_state_table_free", C.c_int, [C.POINTER(GexsStateTable)]),
+    ("gexs_reader_create", C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int,
+                                     C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("gexs_reader_open", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    ("gexs_reader_next", C.c_int, [C.c_void_p] + [C.POINTER(C.c_double)] * 6 +
+     [C.POINTER(C.c_int)]),
+    ("gexs_reader_partition", C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
+    ("gexs_reader_device_lines", C.c_int, [C.c_void_p, C.POINTER(GexsLines)]),
+    ("gexs_reader_close", C.c_int, [C.c_void_p]),
+    ("gexs_reader_destroy", C.c_int, [C.c_void_p]),
     ("gexs_line_table_free", C.c_int, [C.POINTER(GexsLineTable)]),
     ("gexs_manager_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
                                       C.POINTER(C.c_void_p)]),

@@ -29,6 +29,7 @@ SOURCES = [
     "csrc/gexs_ingest.cu",
     "host/B200Manager.cpp",
     "host/gexs_server.cpp",
+    "host/B200ExomolReader.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")
 
@@ -50,6 +51,7 @@ def build(ptxas_verbose=False, force=False):
         deps += [os.path.join(root, f) for f in files]
     deps.append(os.path.join(ROOT, "include", "gexs_b200.h"))
     deps.append(os.path.join(ROOT, "include", "gexs_serve.h"))
+    deps.append(os.path.join(ROOT, "include", "gexs_reader.h"))
     newest = max(os.path.getmtime(d) for d in deps)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
