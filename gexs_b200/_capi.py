@@ -65,6 +65,7 @@ class GexsRequestInfo(C.Structure):
 
 
 BROAD_DEFAULTS, BROAD_BY_J = 0, 1
+OUT_BINARY, OUT_TEXT = 0, 1
 
 
 class GexsStateTable(C.Structure):
@@ -118,6 +119,9 @@ SIGNATURES = [
     ("gexs_state_table_export", C.c_int, [C.POINTER(GexsStateTable)] + [C.c_void_p] * 3),
     ("gexs_line_table_export", C.c_int, [C.POINTER(GexsLineTable)] + [C.c_void_p] * 6),
     ("gexs_state_table_free", C.c_int, [C.POINTER(GexsStateTable)]),
+    ("gexs_write_sigma", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, C.c_int64, C.c_void_p,
+                                   C.c_int]),
     ("gexs_reader_create", C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int,
                                      C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     ("gexs_reader_open", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),

@@ -30,6 +30,7 @@ SOURCES = [
     "host/B200Manager.cpp",
     "host/gexs_server.cpp",
     "host/B200ExomolReader.cpp",
+    "host/gexs_output.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")
 

@@ -266,6 +266,24 @@ int gexs_line_table_export(const gexs_line_table* t, double* d_nu, double* d_elo
 int gexs_state_table_free(gexs_state_table* t);
 int gexs_line_table_free(gexs_line_table* t);
 
+/* ----------------------------------------------------------------- output
+ * One (T, P) cross-section to a file (Profiles/BaseProfile.cpp:269-301
+ * prints every bin with printf on one thread).
+ *  GEXS_OUT_TEXT: exactly the reference's text, "-------T=%12.6f K--------
+ *    P=%12.6f atm---------" and a blank line, then "[%i] %12.6f %13.8E" per
+ *    bin (index, nu_start + double(j)*dnu, sigma_j), then a blank line;
+ *    formatted on nthreads host threads (0 = all) and written in order.
+ *  GEXS_OUT_BINARY: a 64-byte header {char magic[8] = "GEXSSIG1"; int64 n;
+ *    double nu_start, dnu, temperature, pressure; int32 index, reserved;
+ *    int64 pad} then n float64 values.
+ * append != 0 adds to the file (one file per run, as the reference's stdout).
+ * sigma may be host or device memory. */
+#define GEXS_OUT_BINARY 0
+#define GEXS_OUT_TEXT   1
+int gexs_write_sigma(const char* path, int format, int append, int index, double temperature,
+                     double pressure, double nu_start, double dnu, int64_t n,
+                     const double* sigma, int nthreads);
+
 /* ------------------------------------------------------ batched launches
  * A batch owns its device job table and work-item table; launching it is
  * a memset of the work counter plus one persistent kernel per group of
