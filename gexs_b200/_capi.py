@@ -116,6 +116,8 @@ SIGNATURES = [
     ("gexs_exomol_load", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                    C.c_double, C.c_double, C.c_int, C.POINTER(GexsStateTable),
                                    C.POINTER(GexsLineTable)]),
+    ("gexs_hitran_parse", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_double, C.c_double,
+                                    C.c_double, C.c_int, C.POINTER(GexsLineTable)]),
     ("gexs_state_table_export", C.c_int, [C.POINTER(GexsStateTable)] + [C.c_void_p] * 3),
     ("gexs_line_table_export", C.c_int, [C.POINTER(GexsLineTable)] + [C.c_void_p] * 6),
     ("gexs_state_table_free", C.c_int, [C.POINTER(GexsStateTable)]),

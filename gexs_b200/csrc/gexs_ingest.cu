@@ -388,6 +388,67 @@ __global__ void trans_kernel(const uint8_t* __restrict__ text, int64_t nbytes,
     }
 }
 
+/* ---------------------------------------------------------------- HITRAN
+ * 160-column records (Readers/HITRAN/HITRANStateReader.cpp:3-39, 137-250):
+ * field widths {2,1,12,10,10,5,5,10,4,8,15,15,15,15,6,12,1,7,7}; a field is
+ * read by atof/atoi of its columns (bytes past the end of a short line are
+ * absent here; the reference would read stale buffer bytes there). */
+__device__ __forceinline__ double field_atof(const uint8_t* a, const uint8_t* b, int off, int len)
+{
+    const uint8_t* p = a + off;
+    const uint8_t* e = (a + off + len < b) ? a + off + len : b;
+    double v = 0.0;
+    if (p < e) { const uint8_t* q = p; if (!read_double(q, e, &v)) v = 0.0; }
+    return v;
+}
+
+__global__ void hitran_kernel(const uint8_t* __restrict__ text, int64_t nbytes,
+                              const int64_t* __restrict__ line_end, int64_t nlines,
+                              const int64_t* __restrict__ rec, double pressure, double mixture,
+                              double ref_q,
+                              double* __restrict__ nu, double* __restrict__ elow,
+                              double* __restrict__ aif, int32_t* __restrict__ gns,
+                              double* __restrict__ gam, double* __restrict__ nexp)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlines;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t a, b;
+        line_span(line_end, i, nbytes, &a, &b);
+        const uint8_t* p = text + a;
+        const uint8_t* e = text + b;
+        if (!line_has_token(p, e)) continue;
+        const int64_t r = rec[i];
+        const double v_nu = field_atof(p, e, 3, 12);
+        const double v_S = field_atof(p, e, 15, 10);
+        double v_A = field_atof(p, e, 25, 10);
+        const double g_air = field_atof(p, e, 35, 5);
+        const double g_self = field_atof(p, e, 40, 5);
+        const double v_E = field_atof(p, e, 45, 10);
+        const double v_n = field_atof(p, e, 55, 4);
+        double v_g = field_atof(p, e, 146, 7);
+        /* (gam_air*mix + self*(1-mix))*P, HITRANStateReader.cpp:218 */
+        const double gv = __dmul_rn(__dadd_rn(__dmul_rn(g_air, mixture),
+                                              __dmul_rn(g_self, __dsub_rn(1.0, mixture))), pressure);
+        if (v_A == 0.0) {
+            /* A from S at 296 K and Q(296), :222-247 */
+            const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+            const double pi = 3.141592653589793;
+            const double beta = __ddiv_rn(__dmul_rn(planck, vellgt), __dmul_rn(boltz, 296.0));
+            double t = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(v_S, 8.0), pi), vellgt), ref_q), v_nu);
+            t = __dmul_rn(t, v_nu);
+            const double den = __dmul_rn(exp(__dmul_rn(-beta, v_E)), __dsub_rn(1.0, exp(__dmul_rn(-beta, v_nu))));
+            v_A = __ddiv_rn(t, den);
+            v_g = 1.0;
+        }
+        nu[r] = v_nu;
+        elow[r] = v_E;
+        aif[r] = v_A;
+        gns[r] = (int32_t)v_g;
+        gam[r] = gv;
+        nexp[r] = v_n;
+    }
+}
+
 template <typename T>
 __global__ void gather_kernel(const T* __restrict__ in, const int64_t* __restrict__ idx, int64_t n,
                               T* __restrict__ out)
@@ -461,6 +522,57 @@ int index_text(gexs_ctx* ctx, const char* h_text, int64_t nbytes, DevBuf& d_text
     if (e != cudaSuccess) return cuda_error(e, "ingest: index lines");
     *nlines = nl;
     return GEXS_OK;
+}
+
+/* stable radix sort of (nu, record) and a gather of every array */
+int sort_lines(gexs_ctx* ctx, int64_t nrec, DevBuf& nu, DevBuf& el, DevBuf& A, DevBuf& g,
+               DevBuf& gm, DevBuf& nx, cudaStream_t s)
+{
+    const size_t n8 = sizeof(double) * nrec;
+    DevBuf k2, i1, i2, t2;
+    if (k2.alloc(n8) != cudaSuccess || i1.alloc(sizeof(int64_t) * nrec) != cudaSuccess ||
+        i2.alloc(sizeof(int64_t) * nrec) != cudaSuccess)
+        return set_error(GEXS_ERR_OOM, "ingest: sort buffers");
+    iota_kernel<<<grid_for(ctx, nrec, 256), 256, 0, s>>>(i1.as<int64_t>(), nrec);
+    size_t sb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sb, nu.as<double>(), k2.as<double>(), i1.as<int64_t>(),
+                                    i2.as<int64_t>(), nrec, 0, 64, s);
+    if (t2.alloc(sb) != cudaSuccess) return set_error(GEXS_ERR_OOM, "ingest: sort");
+    cub::DeviceRadixSort::SortPairs(t2.p, sb, nu.as<double>(), k2.as<double>(), i1.as<int64_t>(),
+                                    i2.as<int64_t>(), nrec, 0, 64, s);
+    const int gg = grid_for(ctx, nrec, 256);
+    DevBuf tmp;
+    if (tmp.alloc(n8) != cudaSuccess) return set_error(GEXS_ERR_OOM, "ingest: gather");
+    auto regather8 = [&](DevBuf& arr) {
+        gather_kernel<double><<<gg, 256, 0, s>>>(arr.as<double>(), i2.as<int64_t>(), nrec, tmp.as<double>());
+        std::swap(arr.p, tmp.p);
+    };
+    regather8(el); regather8(A); regather8(gm); regather8(nx);
+    gather_kernel<int32_t><<<gg, 256, 0, s>>>(g.as<int32_t>(), i2.as<int64_t>(), nrec, tmp.as<int32_t>());
+    std::swap(g.p, tmp.p);
+    std::swap(nu.p, k2.p);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? GEXS_OK : cuda_error(e, "ingest: sort");
+}
+
+/* records = non-empty lines, numbered in order: rec[i] for line i, *nrec */
+int number_records(gexs_ctx* ctx, const DevBuf& d_text, int64_t nbytes, const DevBuf& d_end,
+                   int64_t nl, DevBuf& d_rec, int64_t* nrec, cudaStream_t s)
+{
+    DevBuf d_flag, d_tmp;
+    if (d_flag.alloc(sizeof(int64_t) * (nl + 1)) != cudaSuccess || d_rec.alloc(sizeof(int64_t) * (nl + 1)) != cudaSuccess)
+        return set_error(GEXS_ERR_OOM, "ingest: record index");
+    cudaMemsetAsync(d_flag.p, 0, sizeof(int64_t) * (nl + 1), s);
+    if (nl > 0)
+        trans_flag_kernel<<<grid_for(ctx, nl, 256), 256, 0, s>>>(d_text.as<uint8_t>(), nbytes,
+                                                                 d_end.as<int64_t>(), nl, d_flag.as<int64_t>());
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, d_flag.as<int64_t>(), d_rec.as<int64_t>(), (int)(nl + 1), s);
+    if (d_tmp.alloc(tb) != cudaSuccess) return set_error(GEXS_ERR_OOM, "ingest: scan");
+    cub::DeviceScan::ExclusiveSum(d_tmp.p, tb, d_flag.as<int64_t>(), d_rec.as<int64_t>(), (int)(nl + 1), s);
+    cudaError_t e = cudaMemcpyAsync(nrec, d_rec.as<int64_t>() + nl, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? GEXS_OK : cuda_error(e, "ingest: count records");
 }
 
 /* "code gamma n J'' [J']" lines; codes other than a0/a1 are skipped */
@@ -631,31 +743,8 @@ int gexs_exomol_parse_trans(gexs_ctx* ctx, const gexs_state_table* states, const
     if (flag & 4) return set_error(GEXS_ERR_INVALID, "gexs_exomol_parse_trans: state id out of range");
 
     if (sort_by_nu && nrec > 1) {
-        /* stable radix sort of (nu, record) and a gather of every array */
-        DevBuf k2, i1, i2, t2;
-        if (k2.alloc(n8) != cudaSuccess || i1.alloc(sizeof(int64_t) * nrec) != cudaSuccess ||
-            i2.alloc(sizeof(int64_t) * nrec) != cudaSuccess)
-            return set_error(GEXS_ERR_OOM, "gexs_exomol_parse_trans: sort buffers");
-        iota_kernel<<<grid_for(ctx, nrec, 256), 256, 0, s>>>(i1.as<int64_t>(), nrec);
-        size_t sb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, sb, nu.as<double>(), k2.as<double>(), i1.as<int64_t>(),
-                                        i2.as<int64_t>(), nrec, 0, 64, s);
-        if (t2.alloc(sb) != cudaSuccess) return set_error(GEXS_ERR_OOM, "gexs_exomol_parse_trans: sort");
-        cub::DeviceRadixSort::SortPairs(t2.p, sb, nu.as<double>(), k2.as<double>(), i1.as<int64_t>(),
-                                        i2.as<int64_t>(), nrec, 0, 64, s);
-        const int gg = grid_for(ctx, nrec, 256);
-        DevBuf tmp;
-        if (tmp.alloc(n8) != cudaSuccess) return set_error(GEXS_ERR_OOM, "gexs_exomol_parse_trans: gather");
-        auto regather8 = [&](DevBuf& arr) {
-            gather_kernel<double><<<gg, 256, 0, s>>>(arr.as<double>(), i2.as<int64_t>(), nrec, tmp.as<double>());
-            std::swap(arr.p, tmp.p);
-        };
-        regather8(el); regather8(A); regather8(gm); regather8(nx);
-        gather_kernel<int32_t><<<gg, 256, 0, s>>>(g.as<int32_t>(), i2.as<int64_t>(), nrec, tmp.as<int32_t>());
-        std::swap(g.p, tmp.p);
-        std::swap(nu.p, k2.p);
-        e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return cuda_error(e, "gexs_exomol_parse_trans: sort");
+        st = sort_lines(ctx, nrec, nu, el, A, g, gm, nx, s);
+        if (st) return st;
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "gexs_exomol_parse_trans");
@@ -692,6 +781,40 @@ int gexs_exomol_load(gexs_ctx* ctx, const char* states_path, const char* trans_p
                                  sort_by_nu, lines_out);
     if (st) { gexs_state_table_free(&S); return st; }
     *states_out = S;
+    return GEXS_OK;
+}
+
+int gexs_hitran_parse(gexs_ctx* ctx, const char* h_text, int64_t nbytes, double pressure,
+                      double air_mixture, double ref_partition_296, int sort_by_nu,
+                      gexs_line_table* out)
+{
+    if (!ctx || !out || nbytes < 0 || (nbytes > 0 && !h_text))
+        return set_error(GEXS_ERR_INVALID, "gexs_hitran_parse: arguments");
+    std::memset(out, 0, sizeof(*out));
+    cudaSetDevice(ctx_device(ctx));
+    cudaStream_t s = 0;
+    DevBuf d_text, d_end, d_rec;
+    int64_t nl = 0, nrec = 0;
+    int st = index_text(ctx, h_text, nbytes, d_text, d_end, &nl, s);
+    if (st) return st;
+    if ((st = number_records(ctx, d_text, nbytes, d_end, nl, d_rec, &nrec, s))) return st;
+    DevBuf nu, el, A, g, gm, nx;
+    const size_t n8 = sizeof(double) * nrec, n4 = sizeof(int32_t) * nrec;
+    if (nu.alloc(n8) != cudaSuccess || el.alloc(n8) != cudaSuccess || A.alloc(n8) != cudaSuccess ||
+        g.alloc(n4) != cudaSuccess || gm.alloc(n8) != cudaSuccess || nx.alloc(n8) != cudaSuccess)
+        return set_error(GEXS_ERR_OOM, "gexs_hitran_parse: line arrays");
+    if (nl > 0)
+        hitran_kernel<<<grid_for(ctx, nl, 256), 256, 0, s>>>(
+            d_text.as<uint8_t>(), nbytes, d_end.as<int64_t>(), nl, d_rec.as<int64_t>(), pressure,
+            air_mixture, ref_partition_296, nu.as<double>(), el.as<double>(), A.as<double>(),
+            g.as<int32_t>(), gm.as<double>(), nx.as<double>());
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "gexs_hitran_parse");
+    if (sort_by_nu && nrec > 1 && (st = sort_lines(ctx, nrec, nu, el, A, g, gm, nx, s))) return st;
+    out->nu = (double*)nu.release(); out->elow = (double*)el.release();
+    out->aif = (double*)A.release(); out->gns = (int32_t*)g.release();
+    out->gamma = (double*)gm.release(); out->n = (double*)nx.release();
+    out->count = nrec;
     return GEXS_OK;
 }
 

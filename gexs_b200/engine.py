@@ -236,6 +236,17 @@ def parse_exomol(ctx, states_text, trans_text, broad_text=b"", broad_mode=capi.B
     return _export_states(st, device), _export_lines(lt, device)
 
 
+def parse_hitran(ctx, text, pressure=1.0, air_mixture=1.0, ref_partition_296=1.0,
+                 sort_by_nu=True, device="cuda"):
+    """HITRAN .par text parsed on the GPU (gexs_hitran_parse): lines dict of
+    torch device tensors."""
+    lt = capi.GexsLineTable()
+    check(lib().gexs_hitran_parse(ctx.h, text, len(text), pressure, air_mixture,
+                                  ref_partition_296, 1 if sort_by_nu else 0, C.byref(lt)),
+          "gexs_hitran_parse")
+    return _export_lines(lt, device)
+
+
 def load_exomol(ctx, states_path, trans_path, broad_path=None, broad_mode=capi.BROAD_DEFAULTS,
                 default_gamma=0.1, default_n=0.1, sort_by_nu=True, device="cuda"):
     """gexs_exomol_load: read the files on the host, parse on the GPU."""

@@ -228,3 +228,35 @@ def make_exomol_transitions(states, ntrans, nu_min, nu_max, seed):
     up = np.minimum(up, hi - 1)
     aif = 10.0 ** rng.uniform(-6.0, 2.0, len(lower))
     return order[up].astype(np.int64), order[lower].astype(np.int64), aif
+
+
+def make_hitran_par(n, seed, nu_min=500.0, nu_max=8000.0, a_zero_every=7):
+    """Seeded HITRAN .par text (160-column records, HITRAN 2004 layout):
+    nu F12.6, S and A E10.3, gamma_air F5.3, gamma_self F5.3, E'' F10.4,
+    n_air F4.2, g' and g'' F7.1; every `a_zero_every`-th record has A = 0
+    (the reader then rebuilds A from S)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nu = np.sort(rng.uniform(nu_min, nu_max, n))
+    S = 10.0 ** rng.uniform(-28.0, -19.0, n)
+    A = 10.0 ** rng.uniform(-6.0, 2.0, n)
+    gair = rng.uniform(0.02, 0.099, n)
+    gself = rng.uniform(0.1, 0.499, n)
+    elow = rng.exponential(1500.0, n)
+    nair = rng.uniform(0.4, 0.8, n)
+    gup = (2 * rng.integers(0, 60, n) + 1).astype(np.float64)
+    glow = (2 * rng.integers(0, 60, n) + 1).astype(np.float64)
+    zero = np.zeros(n, dtype=bool)
+    if a_zero_every:
+        zero[::a_zero_every] = True
+    sci_a = _sci(np.where(zero, 1.0, A), 3)
+    sci_a[zero] = np.frombuffer(b"0.000E+00", dtype=np.uint8)
+    cols = [np.tile(np.frombuffer(b" 11", dtype=np.uint8), (n, 1)),
+            _fixed(nu, 12, 6), _col(n, " "), _sci(S, 3), _col(n, " "), sci_a,
+            _fixed(gair, 5, 3), _fixed(gself, 5, 3), _fixed(elow, 10, 4), _fixed(nair, 4, 2),
+            np.tile(np.frombuffer(b" 0.00000", dtype=np.uint8), (n, 1)),
+            np.full((n, 60), ord(" "), dtype=np.uint8),
+            np.tile(np.frombuffer(b"000000" + b"0" * 12 + b" ", dtype=np.uint8), (n, 1)),
+            _fixed(gup, 7, 1), _fixed(glow, 7, 1), _col(n, "\n")]
+    rows = np.hstack(cols)
+    assert rows.shape[1] == 161
+    return rows.tobytes()

@@ -258,6 +258,18 @@ int gexs_exomol_load(gexs_ctx* ctx, const char* states_path, const char* trans_p
                      const char* broad_path, int broad_mode, double default_gamma,
                      double default_n, int sort_by_nu, gexs_state_table* states_out,
                      gexs_line_table* lines_out);
+/* HITRAN .par text (Readers/HITRAN/HITRANStateReader.cpp:137-250) parsed on
+ * the GPU, one thread per 160-column record: nu, S, A, gamma_air,
+ * gamma_self, E'', n_air and g' by atof of their columns; gamma =
+ * (gamma_air*air_mixture + gamma_self*(1-air_mixture))*pressure (:218);
+ * where A == 0, A = S*8*pi*c*Q(296)*nu^2/(exp(-c2 E''/296)*(1-exp(-c2
+ * nu/296))) and g' = 1 (:222-247).  Q(296) is the caller's: the reference
+ * takes it from the TIPS-2011 Fortran tables (BD_TIPS_2011_v1p0.for), which
+ * this library does not carry. */
+int gexs_hitran_parse(gexs_ctx* ctx, const char* h_text, int64_t nbytes, double pressure,
+                      double air_mixture, double ref_partition_296, int sort_by_nu,
+                      gexs_line_table* out);
+
 /* copy a table into caller-owned device arrays of `count` elements */
 int gexs_state_table_export(const gexs_state_table* t, double* d_energy, int32_t* d_g,
                             int32_t* d_J);

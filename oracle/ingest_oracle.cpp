@@ -16,7 +16,9 @@
  *                      (the key keeps the failed "a1" text after
  *                      key.clear(), :21); mode 1 the intended rule: "a1"
  *                      (J'', J'), then "a0" (J''), then the defaults.
- * Pinned by tests/test_ingest_pin.py against the reference reader compiled
+ *   orc_hitran         Readers/HITRAN/HITRANStateReader.cpp:137-250 (see
+ *                      the function).
+ * Pinned by tests/test_ingest_pin.py against the reference readers compiled
  * from its own sources (oracle/_ref/gexsref_reader).  Written with libc
  * only (no iostreams): `>> int` is restated as whitespace, sign, decimal
  * digits (failing on none or on int overflow) and `>> double` as the
@@ -27,6 +29,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <string>
@@ -181,6 +184,57 @@ int64_t orc_exomol_trans(const char* text, int64_t n, const double* sE, const in
             gns[k] = sg[f];
             gam[k] = gv;
             nexp[k] = xv;
+        }
+        ++k;
+    }
+    return k;
+}
+
+/* Readers/HITRAN/HITRANStateReader.cpp:137-250 restated: one record per
+ * non-empty line; fields by atof of their columns (:21-29, widths
+ * {2,1,12,10,10,5,5,10,4,8,15,15,15,15,6,12,1,7,7}); gamma = (gamma_air*mix
+ * + gamma_self*(1-mix))*P; where A == 0 it is rebuilt from S with Q(296)
+ * = ref_q and g' = 1.  Columns past the end of a short line are treated as
+ * absent (the reference reads stale buffer bytes there). */
+static double col_atof(const char* line, int64_t len, int off, int w)
+{
+    char f[13] = {0};
+    const int64_t n = std::min<int64_t>(w, std::max<int64_t>(0, len - off));
+    if (n > 0) std::memcpy(f, line + off, (size_t)n);
+    return std::atof(f);
+}
+
+int64_t orc_hitran(const char* text, int64_t n, double pressure, double mixture, double ref_q,
+                   double* nu, double* elow, double* aif, int32_t* gns, double* gam,
+                   double* nexp, int64_t cap)
+{
+    int64_t i = 0, k = 0;
+    while (i < n) {
+        int64_t j = i;
+        while (j < n && text[j] != '\n') ++j;
+        const char* line = text + i;
+        const int64_t len = j - i;
+        i = j + 1;
+        bool blank = true;
+        for (int64_t t = 0; t < len; ++t) if (!is_ws(line[t])) { blank = false; break; }
+        if (blank) continue;
+        const double v_nu = col_atof(line, len, 3, 12), v_S = col_atof(line, len, 15, 10);
+        double v_A = col_atof(line, len, 25, 10);
+        const double g_air = col_atof(line, len, 35, 5), g_self = col_atof(line, len, 40, 5);
+        const double v_E = col_atof(line, len, 45, 10), v_n = col_atof(line, len, 55, 4);
+        double v_g = col_atof(line, len, 146, 7);
+        const double gv = (g_air * mixture + g_self * (1.0 - mixture)) * pressure;
+        if (v_A == 0.0) {
+            const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+            const double pi = std::acos(-1.0);
+            const double beta = planck * vellgt / (boltz * 296.0);
+            v_A = v_S * 8.0 * pi * vellgt * ref_q * v_nu * v_nu /
+                  (std::exp(-beta * v_E) * (1.0 - std::exp(-beta * v_nu)));
+            v_g = 1.0;
+        }
+        if (k < cap) {
+            nu[k] = v_nu; elow[k] = v_E; aif[k] = v_A; gns[k] = (int32_t)v_g;
+            gam[k] = gv; nexp[k] = v_n;
         }
         ++k;
     }

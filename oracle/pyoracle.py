@@ -61,6 +61,9 @@ def orc():
                                         C.c_double] + [C.c_void_p] * 6 + [C.c_int64])
         h.orc_sort_by_nu.restype = None
         h.orc_sort_by_nu.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        h.orc_hitran.restype = C.c_int64
+        h.orc_hitran.argtypes = [C.c_char_p, C.c_int64, C.c_double, C.c_double, C.c_double] + \
+            [C.c_void_p] * 6 + [C.c_int64]
         h.orc_strtod.restype = C.c_double
         h.orc_strtod.argtypes = [C.c_char_p]
         _orc = h
@@ -216,6 +219,39 @@ def ref_exomol_read(states_path, trans_path, broad_path=None, default_gamma=0.1,
         subprocess.run([REF_READER_BIN, states_path, trans_path, broad_path or "-",
                         repr(float(default_gamma)), repr(float(default_n)), out], check=True,
                        stdout=subprocess.DEVNULL)
+        raw = np.fromfile(out, dtype=np.uint8)
+    n = int(raw[:8].view(np.int64)[0])
+    arr = raw[8:].view(np.float64).reshape(6, n) if n else np.zeros((6, 0))
+    keys = ("nu", "gns", "elow", "aif", "gamma", "n")
+    return {k: arr[i].copy() for i, k in enumerate(keys)}
+
+
+def hitran(text, pressure=1.0, mixture=1.0, ref_q=1.0, sort_by_nu=False):
+    """Restated HITRANStateReader.cpp:137-250 (Q(296) = ref_q)."""
+    h = orc()
+    args = (text, len(text), pressure, mixture, ref_q)
+    n = h.orc_hitran(*args, None, None, None, None, None, None, 0)
+    d = {k: np.zeros(n, np.float64) for k in ("nu", "elow", "aif", "gamma", "n")}
+    d["gns"] = np.zeros(n, np.int32)
+    h.orc_hitran(*args, _p(d["nu"]), _p(d["elow"]), _p(d["aif"]), _p(d["gns"]), _p(d["gamma"]),
+                 _p(d["n"]), n)
+    if sort_by_nu and n:
+        perm = np.zeros(n, np.int64)
+        h.orc_sort_by_nu(_p(d["nu"]), n, _p(perm))
+        d = {k: v[perm] for k, v in d.items()}
+    return d
+
+
+def ref_hitran_read(path, pressure=1.0, mixture=1.0, ref_q=1.0):
+    """The reference's HITRANStateReader (compiled from its sources, TIPS
+    replaced by the constant ref_q): every record in file order as
+    (nu, gns, e_i, aif, gamma, n)."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "ref.bin")
+        subprocess.run([REF_READER_BIN, "hitran", path, repr(float(pressure)), repr(float(mixture)),
+                        repr(float(ref_q)), out], check=True, stdout=subprocess.DEVNULL)
         raw = np.fromfile(out, dtype=np.uint8)
     n = int(raw[:8].view(np.int64)[0])
     arr = raw[8:].view(np.float64).reshape(6, n) if n else np.zeros((6, 0))

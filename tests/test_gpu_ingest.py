@@ -154,3 +154,23 @@ def test_load_files_then_cross_section(gpu_ctx, tmp_path):
     want = po.cross_section(H.host_job(jb.c, host))
     worst, nbad = H.fp64_mismatch(out.cpu().numpy(), want)
     assert nbad == 0, worst
+
+
+@pytest.mark.parametrize("sort", [False, True])
+def test_hitran_matches_oracle(gpu_ctx, sort):
+    """gexs_hitran_parse against the restated HITRANStateReader (pinned to
+    the reference in test_ingest_pin.py): nu, E'', gamma, n, g' bit-exact, A
+    bit-exact where the file gives it; where it is rebuilt from S the GPU's
+    FP64 exp stands in for glibc's: within 4 ulp."""
+    from gexs_b200.engine import parse_hitran
+    text = synth.make_hitran_par(30000, 89)
+    got = parse_hitran(gpu_ctx, text, pressure=0.8, air_mixture=0.7, ref_partition_296=174.58,
+                       sort_by_nu=sort)
+    ref = po.hitran(text, 0.8, 0.7, 174.58, sort_by_nu=sort)
+    for k in ("nu", "elow", "gamma", "n", "gns"):
+        assert _bits_equal(got[k].cpu().numpy(), ref[k]), k
+    a, b = got["aif"].cpu().numpy(), ref["aif"]
+    rebuilt = ref["gns"] == 1
+    assert _bits_equal(a[~rebuilt], b[~rebuilt])
+    ulp = np.spacing(np.abs(b[rebuilt]))
+    assert (np.abs(a[rebuilt] - b[rebuilt]) <= 4 * ulp).all()

@@ -101,3 +101,22 @@ def test_states_energies_are_strtod(tmp_path):
     expect = np.array([float(ln.split()[1]) for ln in stext.splitlines()])
     assert np.array_equal(e.view(np.int64), expect.view(np.int64))
     assert np.array_equal(g, st.g) and np.array_equal(j, st.j)
+
+
+def test_hitran_oracle_matches_reference_reader(tmp_path):
+    """HITRANStateReader compiled from its sources (TIPS replaced by a
+    constant Q(296), the Fortran being unbuildable here): nu, E'', g', n and
+    gamma bit-exact; A bit-exact where the file has it, and within 4 ulp
+    where the reader rebuilds it from S (glibc exp on both sides, the same
+    operation order)."""
+    text = synth.make_hitran_par(4000, 83)
+    p = _write(tmp_path, "h.par", text)
+    ref = po.ref_hitran_read(p, pressure=0.8, mixture=0.7, ref_q=174.58)
+    orc = po.hitran(text, pressure=0.8, mixture=0.7, ref_q=174.58)
+    assert len(orc["nu"]) == 4000 and len(ref["nu"]) == 4000
+    for k in ("nu", "elow", "gamma", "n"):
+        assert np.array_equal(ref[k].view(np.int64), orc[k].view(np.int64)), k
+    assert np.array_equal(ref["gns"], orc["gns"].astype(np.float64))
+    assert np.array_equal(ref["aif"].view(np.int64), orc["aif"].view(np.int64))
+    rebuilt = np.arange(4000) % 7 == 0
+    assert (orc["gns"][rebuilt] == 1).all() and (orc["aif"][rebuilt] > 0).all()
