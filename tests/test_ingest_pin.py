@@ -1,7 +1,7 @@
 """Pin the CPU restatement of the ExoMol reader (oracle/ingest_oracle.cpp)
 to the reference's own reader, compiled from its sources
 (Readers/Exomol/ExomolStateReader.cpp, exomol_functions.cpp, common/Util.cpp
--> oracle/_ref/libgexsref_reader.so), on seeded synthetic files.  Runs on
+-> oracle/_ref/gexsref_reader), on seeded synthetic files.  Runs on
 the CPU; the GPU ingest is checked against the oracle in test_gpu_ingest.py.
 """
 import os
