@@ -522,8 +522,9 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
  * distance from the centre.  Region I: x (FFMA2), m = x^2 + y^2 - 1/2
  * (FFMA2), d = m^2 + 2 y^2 (FFMA2), two MUFU reciprocals, t = (m + 1)/d
  * (FFMA2), accumulate a t (FFMA2), n += 64 (FADD2): 6 packed FP32 issues and
- * 2 MUFU per pair of bins.  Records are taken two at a time so their loads
- * and arithmetic overlap; a bin still sums its lines in ascending order. */
+ * 2 MUFU per pair of bins.  Records are taken four (else two) at a time, all
+ * their constants loaded first, so loads and arithmetic of several lines
+ * overlap; a bin still sums its lines in ascending order. */
 template <int B>
 __device__ __forceinline__ void voigt_full2(const RecV& p, const RecV& q, float2 lw2,
                                             float2 (&part)[B / 2])
@@ -605,6 +606,21 @@ __device__ __forceinline__ void voigt_one(const RecV& q, int tier, int wb, int l
     }
 }
 
+/* four full-tier records: every constant loaded first, then two pairs */
+template <int B>
+__device__ __forceinline__ void voigt_full4(const RecV* __restrict__ r, float2 lw2,
+                                            float2 (&part)[B / 2])
+{
+    RecV q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        q[k].dx = r[k].dx; q[k].mf = r[k].mf; q[k].c = r[k].c;
+        q[k].y2 = r[k].y2; q[k].a = r[k].a; q[k].nb = r[k].nb;
+    }
+    voigt_full2<B>(q[0], q[1], lw2, part);
+    voigt_full2<B>(q[2], q[3], lw2, part);
+}
+
 template <int B>
 __device__ __forceinline__ void lines_voigt_f32(const RecV* __restrict__ rec, int nrec, int warp,
                                                 int lane, float2 (&part)[B / 2])
@@ -613,6 +629,21 @@ __device__ __forceinline__ void lines_voigt_f32(const RecV* __restrict__ rec, in
     const float lw = (float)(wb + lane);
     const float2 lw2 = make_float2(lw, lw);
     int i = 0;
+    for (; i + 3 < nrec; i += 4) {
+        const int t0 = (rec[i].tiers >> sh) & 3, t1 = (rec[i + 1].tiers >> sh) & 3;
+        const int t2 = (rec[i + 2].tiers >> sh) & 3, t3 = (rec[i + 3].tiers >> sh) & 3;
+        if (t0 == 1 && t1 == 1 && t2 == 1 && t3 == 1) { voigt_full4<B>(rec + i, lw2, part); continue; }
+        if (t0 == 1 && t1 == 1) voigt_full2<B>(rec[i], rec[i + 1], lw2, part);
+        else {
+            if (t0) voigt_one<B>(rec[i], t0, wb, lane, lw2, part);
+            if (t1) voigt_one<B>(rec[i + 1], t1, wb, lane, lw2, part);
+        }
+        if (t2 == 1 && t3 == 1) voigt_full2<B>(rec[i + 2], rec[i + 3], lw2, part);
+        else {
+            if (t2) voigt_one<B>(rec[i + 2], t2, wb, lane, lw2, part);
+            if (t3) voigt_one<B>(rec[i + 3], t3, wb, lane, lw2, part);
+        }
+    }
     for (; i + 1 < nrec; i += 2) {
         const int tp = (rec[i].tiers >> sh) & 3, tq = (rec[i + 1].tiers >> sh) & 3;
         if (tp == 1 && tq == 1) { voigt_full2<B>(rec[i], rec[i + 1], lw2, part); continue; }
