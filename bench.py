@@ -652,9 +652,10 @@ def our_arm(args):
                                       "grid-slices x%d" % ws,
                        "l2": "inputs (%.1f GB of lines) larger than L2" % (line_bytes / 1e9),
                        "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]}},
-            # per step: prep_kernel (S(T), width, y per line), voigt_ws_kernel
-            # (region I) and core_kernel (Humlicek regions II-IV)
-            "gpu_launches": 3 * args.steps,
+            # per step: put_blob_kernel (launch table), prep_kernel (S(T),
+            # width, y per line), voigt_ws_kernel (region I), zero_ints_kernel
+            # (core work counter) and core_kernel (Humlicek regions II-IV)
+            "gpu_launches": 5 * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": traffic,

@@ -71,6 +71,10 @@ struct gexs_ctx {
     int device = 0;
     int nsm = 148;
     int* d_err = nullptr;            /* sticky kernel error word */
+    /* launch tables and per-line prep arrays: kept mapped between calls (no
+     * release threshold) and never made to wait on a free from another
+     * stream (no internal dependencies), so calls on two streams overlap */
+    cudaMemPool_t pool = nullptr;
     std::mutex mu;
     std::map<int, gexs_launch_cfg> tuned;   /* key: pk*4 + prec */
 };
@@ -319,6 +323,23 @@ int gexs_ctx_create(int device, gexs_ctx** out)
     e = cudaMalloc(&c->d_err, sizeof(int));
     if (e != cudaSuccess) { delete c; return set_error(GEXS_ERR_OOM, "error word"); }
     cudaMemset(c->d_err, 0, sizeof(int));
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        int no = 0;
+        if (cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
+            cudaMemPoolSetAttribute(c->pool, cudaMemPoolReuseAllowInternalDependencies, &no) != cudaSuccess) {
+            cudaMemPoolDestroy(c->pool);
+            c->pool = nullptr;
+        }
+    } else {
+        c->pool = nullptr;
+    }
+    cudaGetLastError();
     *out = c;
     return GEXS_OK;
 }
@@ -328,6 +349,7 @@ int gexs_ctx_destroy(gexs_ctx* ctx)
     if (!ctx) return GEXS_OK;
     cudaSetDevice(ctx->device);
     cudaFree(ctx->d_err);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return GEXS_OK;
 }
@@ -361,11 +383,12 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
         const bool prep = !(cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
         Layout L = group_layout(g, prep);
         void* d = nullptr;
-        e = cudaMallocAsync(&d, L.bytes, s);
+        e = ctx->pool ? cudaMallocFromPoolAsync(&d, L.bytes, ctx->pool, s)
+                      : cudaMallocAsync(&d, L.bytes, s);
         if (e != cudaSuccess) return set_error(GEXS_ERR_OOM, "launch tables");
+        /* the image carries the zeroed work counters */
         std::vector<unsigned char> h = group_image(g, L, (unsigned char*)d, prep);
-        e = cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync((unsigned char*)d + L.oc, 0, sizeof(int), s);
+        e = put_bytes(d, h.data(), h.size(), s);
         if (e != cudaSuccess) { cudaFreeAsync(d, s); return cuda_error(e, "upload launch tables"); }
         e = enqueue_group(g, L, (unsigned char*)d, prep, cfgs[gi], ctx->d_err, ctx->nsm, s);
         cudaFreeAsync(d, s);
@@ -418,7 +441,7 @@ static int batch_enqueue(gexs_batch* b, cudaStream_t s)
         const Group& g = b->groups[gi];
         if (g.nitems == 0) continue;
         unsigned char* d = (unsigned char*)b->dmem[gi];
-        cudaError_t e = cudaMemsetAsync(d + b->layouts[gi].oc, 0, sizeof(int), s);
+        cudaError_t e = zero_ints((int*)(d + b->layouts[gi].oc), 1, s);
         if (e != cudaSuccess) return cuda_error(e, "reset work counter");
         e = enqueue_group(g, b->layouts[gi], d, b->prep[gi], b->cfgs[gi], b->ctx->d_err,
                           b->ctx->nsm, s);

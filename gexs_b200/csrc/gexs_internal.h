@@ -13,7 +13,8 @@ int tile_bins(const gexs_launch_cfg& c);
 /* d_prep: device array of per-job prep arrays (S | invw | y, 3 N doubles
  * each, from launch_prep), or NULL to derive every line on load.
  * d_counter: a 256-byte block of work counters; the caller zeroes the
- * first int, the FP32 Voigt core kernel's counter (int 32) is zeroed here. */
+ * first int, the FP32 Voigt core kernel's counter (int 32) is zeroed here
+ * (by zero_ints). */
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
@@ -25,6 +26,14 @@ cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* 
 cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,
                              const double* d_betas, int nt, double* d_partial, int nchunk,
                              double* d_q, cudaStream_t st);
+
+/* small control writes done by kernels (gexs_kernels.cu): a launch table
+ * passed as kernel parameters (at most kMaxParamUpload bytes) and zeroed
+ * work counters, so that they never queue on a copy engine behind bulk
+ * host-to-device copies of lines running on another stream */
+const size_t kMaxParamUpload = 64 * 1024;
+cudaError_t put_bytes(void* dst, const void* src, size_t n, cudaStream_t st);
+cudaError_t zero_ints(int* p, int n, cudaStream_t st);
 
 /* context accessors (gexs_capi.cu) */
 int ctx_device(gexs_ctx* c);

@@ -3,6 +3,7 @@
  * Q(T), and the front of the tile-kernel dispatch (the tile kernel itself
  * is in gexs_tiles.cuh).
  */
+#include <cstring>
 #include "gexs_tiles.cuh"
 
 namespace gexs {
@@ -137,6 +138,44 @@ cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs
 }
 
 int tile_bins(const gexs_launch_cfg& c) { return 32 * c.bins_per_lane * c.warps; }
+
+/* ----------------------------------------------- control writes as kernels */
+namespace {
+const int kBlobBytes = 4000;                /* under the 4 KB kernel-parameter limit */
+struct Blob { unsigned char b[kBlobBytes]; };
+
+__global__ void put_blob_kernel(const Blob p, unsigned char* dst, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = p.b[i];
+}
+
+__global__ void zero_ints_kernel(int* p, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0;
+}
+}  // namespace
+
+cudaError_t put_bytes(void* dst, const void* src, size_t n, cudaStream_t st)
+{
+    if (n > kMaxParamUpload) return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st);
+    const unsigned char* s = static_cast<const unsigned char*>(src);
+    unsigned char* d = static_cast<unsigned char*>(dst);
+    for (size_t o = 0; o < n; o += kBlobBytes) {
+        const int k = (int)std::min<size_t>(kBlobBytes, n - o);
+        Blob b;
+        std::memcpy(b.b, s + o, (size_t)k);
+        put_blob_kernel<<<1, 256, 0, st>>>(b, d + o, k);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t zero_ints(int* p, int n, cudaStream_t st)
+{
+    zero_ints_kernel<<<1, 64, 0, st>>>(p, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,
                          int nsm, cudaStream_t st)

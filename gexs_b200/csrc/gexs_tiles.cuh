@@ -1460,7 +1460,7 @@ static cudaError_t launch_core(const KArgs& a, int nsm, cudaStream_t st)
     const int grid = max(1, min(a.nitems, max(occ, 1) * nsm));
     KArgs c = a;
     c.counter = a.counter + CORE_COUNTER_OFFSET;
-    e = cudaMemsetAsync(c.counter, 0, sizeof(int), st);
+    e = zero_ints(c.counter, 1, st);
     if (e != cudaSuccess) return e;
     kern<<<grid, CORE_WARPS * 32, smem, st>>>(c);
     return cudaGetLastError();

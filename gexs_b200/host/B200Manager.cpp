@@ -4,10 +4,20 @@
  */
 #include "B200Manager.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
 #include <cuda_runtime.h>
+
+namespace {
+const int kCopyChunks = 32;                     /* pieces of an overlapped line copy */
+const int kSegments = 5;                        /* grid segments of the first launch  */
+const double kSegmentFrac[kSegments] = {1.0 / 32, 1.0 / 8, 1.0 / 4, 1.0 / 2, 1.0};
+const int64_t kSegmentAlign = 4096;             /* widest tile: 32 lanes x 16 bins x 8 warps */
+const size_t kSegmentMinLines = (size_t)1 << 21;
+const size_t kSamples = 8192;
+}  // namespace
 
 B200Manager::B200Manager(ProfileType profile, int device, int convention, int precision,
                          size_t memory_bytes)
@@ -16,9 +26,24 @@ B200Manager::B200Manager(ProfileType profile, int device, int convention, int pr
 {
     int st = gexs_ctx_create(device, &ctx_);
     if (st) { fail(st); return; }
-    cudaStream_t s;
+    cudaStream_t s, cs;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
     stream_ = (void*)s;
+    for (int k = 1; k < kSegments; ++k) {
+        cudaStream_t sk;
+        if (cudaStreamCreateWithFlags(&sk, cudaStreamNonBlocking) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
+        seg_stream_.push_back((void*)sk);
+    }
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
+    copy_stream_ = (void*)cs;
+    for (int c = 0; c < kCopyChunks + kSegments + 1; ++c) {
+        cudaEvent_t e;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
+        if (c < kCopyChunks) chunk_ev_.push_back((void*)e);
+        else if (c == kCopyChunks) done_ev_ = (void*)e;
+        else if (c == kCopyChunks + 1) fork_ev_ = (void*)e;
+        else join_ev_.push_back((void*)e);
+    }
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     if (memory_bytes_ == 0) memory_bytes_ = fr / 2;
@@ -28,6 +53,12 @@ B200Manager::B200Manager(ProfileType profile, int device, int convention, int pr
 B200Manager::~B200Manager()
 {
     Cleanup();
+    for (void* e : chunk_ev_) cudaEventDestroy((cudaEvent_t)e);
+    for (void* e : join_ev_) cudaEventDestroy((cudaEvent_t)e);
+    for (void* e : {done_ev_, fork_ev_})
+        if (e) cudaEventDestroy((cudaEvent_t)e);
+    if (copy_stream_) cudaStreamDestroy((cudaStream_t)copy_stream_);
+    for (void* sk : seg_stream_) cudaStreamDestroy((cudaStream_t)sk);
     if (stream_) cudaStreamDestroy((cudaStream_t)stream_);
     gexs_ctx_destroy(ctx_);
 }
@@ -100,17 +131,63 @@ void B200Manager::TransferVectors(size_t Nener, double* h_energies, double* h_nu
     if (flush()) return;
     if (Nener > N_trans) { fail(GEXS_ERR_INVALID); return; }
     cudaSetDevice(device_);
-    cudaStream_t s = (cudaStream_t)stream_;
+    cudaStream_t cs = (cudaStream_t)copy_stream_;
     tasks_ = 0;
     nlines_ = Nener;
-    bool ok = cudaMemcpyAsync(d_e_, h_energies, sizeof(double) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-              cudaMemcpyAsync(d_nu_, h_nu, sizeof(double) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-              cudaMemcpyAsync(d_a_, h_aif, sizeof(double) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-              cudaMemcpyAsync(d_g_, h_gns, sizeof(int) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess;
-    if (ok && h_gamma && h_n && d_gam_ && d_n_)
-        ok = cudaMemcpyAsync(d_gam_, h_gamma, sizeof(double) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-             cudaMemcpyAsync(d_n_, h_n, sizeof(double) * Nener, cudaMemcpyHostToDevice, s) == cudaSuccess;
-    if (!ok) fail(GEXS_ERR_CUDA);
+    /* kernels queued on the previous lines must finish before they are overwritten */
+    if (cudaEventRecord((cudaEvent_t)done_ev_, (cudaStream_t)stream_) != cudaSuccess ||
+        cudaStreamWaitEvent(cs, (cudaEvent_t)done_ev_, 0) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
+    const bool press = h_gamma && h_n && d_gam_ && d_n_;
+    nchunks_ = Nener == 0 ? 0 : (Nener >= kSegmentMinLines ? kCopyChunks : 1);
+    chunk_lines_ = nchunks_ ? (Nener + nchunks_ - 1) / nchunks_ : 0;
+    bool ok = true;
+    for (int c = 0; c < nchunks_ && ok; ++c) {
+        const size_t i0 = std::min(Nener, (size_t)c * chunk_lines_);
+        const size_t n = std::min(chunk_lines_, Nener - i0);
+        const size_t d8 = sizeof(double) * n, d4 = sizeof(int) * n;
+        if (n) {
+            ok = cudaMemcpyAsync(d_nu_ + i0, h_nu + i0, d8, cudaMemcpyHostToDevice, cs) == cudaSuccess &&
+                 cudaMemcpyAsync(d_e_ + i0, h_energies + i0, d8, cudaMemcpyHostToDevice, cs) == cudaSuccess &&
+                 cudaMemcpyAsync(d_a_ + i0, h_aif + i0, d8, cudaMemcpyHostToDevice, cs) == cudaSuccess &&
+                 cudaMemcpyAsync(d_g_ + i0, h_gns + i0, d4, cudaMemcpyHostToDevice, cs) == cudaSuccess;
+            if (ok && press)
+                ok = cudaMemcpyAsync(d_gam_ + i0, h_gamma + i0, d8, cudaMemcpyHostToDevice, cs) == cudaSuccess &&
+                     cudaMemcpyAsync(d_n_ + i0, h_n + i0, d8, cudaMemcpyHostToDevice, cs) == cudaSuccess;
+        }
+        if (ok) ok = cudaEventRecord((cudaEvent_t)chunk_ev_[c], cs) == cudaSuccess;
+    }
+    if (!ok) { fail(GEXS_ERR_CUDA); return; }
+    /* nu at every stride-th line and at the last: conservative line bounds later */
+    samp_idx_.clear(); samp_nu_.clear();
+    if (Nener) {
+        const size_t stride = std::max<size_t>(1, Nener / kSamples);
+        for (size_t i = 0; i < Nener; i += stride) { samp_idx_.push_back(i); samp_nu_.push_back(h_nu[i]); }
+        if (samp_idx_.back() != Nener - 1) { samp_idx_.push_back(Nener - 1); samp_nu_.push_back(h_nu[Nener - 1]); }
+    }
+    fresh_ = nchunks_ > 0;
+}
+
+/* first index whose nu can be >= v: lines before it all have nu < v */
+size_t B200Manager::lines_below(double v) const
+{
+    auto it = std::lower_bound(samp_nu_.begin(), samp_nu_.end(), v);   /* first sample >= v */
+    if (it == samp_nu_.begin()) return 0;
+    return samp_idx_[(size_t)(it - samp_nu_.begin()) - 1];
+}
+
+/* an index past every line with nu <= v */
+size_t B200Manager::lines_upto(double v) const
+{
+    auto it = std::upper_bound(samp_nu_.begin(), samp_nu_.end(), v);   /* first sample > v */
+    if (it == samp_nu_.end()) return nlines_;
+    return samp_idx_[(size_t)(it - samp_nu_.begin())];
+}
+
+/* nu of the sampled line at or below index i */
+double B200Manager::nu_at(size_t i) const
+{
+    auto it = std::upper_bound(samp_idx_.begin(), samp_idx_.end(), i);
+    return samp_nu_[(size_t)(it - samp_idx_.begin()) - 1];
 }
 
 void B200Manager::ExecuteCrossSection(int, int, int)
@@ -146,10 +223,91 @@ void B200Manager::ExecuteCrossSection(int N, int N_ener, int start_idx, double t
 int B200Manager::flush()
 {
     if (pending_.empty()) return status_;
-    int st = gexs_run(ctx_, pending_.data(), (int)pending_.size(), nullptr, stream_);
+    int st = fresh_ ? run_segmented()
+                    : gexs_run(ctx_, pending_.data(), (int)pending_.size(), nullptr, stream_);
     pending_.clear();
     if (st) return fail(st);
     return GEXS_OK;
+}
+
+/* The queued pairs right after TransferVectors: grid segments at the line
+ * quantiles kSegmentFrac, each given the sub-list of lines that can reach
+ * it (every line within cutoff + margin of its bins, a superset of what
+ * each tile's own search selects, so each tile finds the same lines in the
+ * same order) and started once the pieces holding that sub-list have
+ * arrived.  Segment boundaries sit at start_idx + k * kSegmentAlign, so
+ * every tile is the tile of a single launch over the pair. */
+int B200Manager::run_segmented()
+{
+    cudaStream_t s0 = (cudaStream_t)stream_;
+    std::vector<std::vector<gexs_job>> seg(kSegments);
+    std::vector<size_t> need(kSegments, 0);
+    for (const gexs_job& j : pending_) {
+        const size_t ne = (size_t)j.lines.count;
+        const int64_t S = j.start_idx, E = j.start_idx + j.n_points;
+        if (ne < kSegmentMinLines || j.n_points < 2 * kSegmentAlign || samp_nu_.empty()) {
+            seg[kSegments - 1].push_back(j);
+            need[kSegments - 1] = std::max(need[kSegments - 1], ne);
+            continue;
+        }
+        int64_t b0 = S;
+        for (int k = 0; k < kSegments && b0 < E; ++k) {
+            int64_t b1 = E;
+            if (k + 1 < kSegments) {
+                const double nu = nu_at((size_t)(kSegmentFrac[k] * (double)(ne - 1)));
+                const double bin = std::floor((nu - j.nu_start) / j.dnu);
+                if (bin > (double)S) {
+                    const int64_t g = S + ((std::min((int64_t)bin, E) - S) / kSegmentAlign) * kSegmentAlign;
+                    b1 = std::max(b0, g);
+                } else {
+                    b1 = b0;
+                }
+                if (b1 == b0) continue;
+            }
+            const double f0 = j.nu_start + (double)b0 * j.dnu;
+            const double fl = j.nu_start + (double)(b1 - 1) * j.dnu;
+            const double m = 8.0 * j.dnu + 1e-8 * (std::fabs(fl) + j.cutoff);
+            size_t L0 = std::min(lines_below(f0 - j.cutoff - m), ne);
+            size_t L1 = std::min(lines_upto(fl + j.cutoff + m), ne);
+            L0 &= ~(size_t)3;
+            if (L1 < L0) L1 = L0;
+            gexs_job p = j;
+            p.start_idx = b0;
+            p.n_points = b1 - b0;
+            p.lines.nu = j.lines.nu + L0; p.lines.elow = j.lines.elow + L0;
+            p.lines.aif = j.lines.aif + L0; p.lines.gns = j.lines.gns + L0;
+            if (j.lines.gamma) p.lines.gamma = j.lines.gamma + L0;
+            if (j.lines.n) p.lines.n = j.lines.n + L0;
+            p.lines.count = (int64_t)(L1 - L0);
+            seg[k].push_back(p);
+            need[k] = std::max(need[k], L1);
+            b0 = b1;
+        }
+    }
+    fresh_ = false;
+    /* segment k runs on stream k (stream_ for the first), forked from stream_ */
+    if (cudaEventRecord((cudaEvent_t)fork_ev_, s0) != cudaSuccess) return GEXS_ERR_CUDA;
+    for (void* sk : seg_stream_)
+        if (cudaStreamWaitEvent((cudaStream_t)sk, (cudaEvent_t)fork_ev_, 0) != cudaSuccess)
+            return GEXS_ERR_CUDA;
+    int st = GEXS_OK;
+    for (int k = 0; k < kSegments && st == GEXS_OK; ++k) {
+        if (seg[k].empty()) continue;
+        cudaStream_t s = k == 0 ? s0 : (cudaStream_t)seg_stream_[k - 1];
+        if (need[k] > 0) {
+            const size_t c = std::min((size_t)nchunks_ - 1, (need[k] - 1) / chunk_lines_);
+            if (cudaStreamWaitEvent(s, (cudaEvent_t)chunk_ev_[c], 0) != cudaSuccess) { st = GEXS_ERR_CUDA; break; }
+        }
+        st = gexs_run(ctx_, seg[k].data(), (int)seg[k].size(), nullptr, s);
+    }
+    /* stream_ joins every segment stream and has seen every piece arrive */
+    bool ok = true;
+    for (size_t k = 0; k < seg_stream_.size() && ok; ++k)
+        ok = cudaEventRecord((cudaEvent_t)join_ev_[k], (cudaStream_t)seg_stream_[k]) == cudaSuccess &&
+             cudaStreamWaitEvent(s0, (cudaEvent_t)join_ev_[k], 0) == cudaSuccess;
+    if (ok) ok = cudaStreamWaitEvent(s0, (cudaEvent_t)chunk_ev_[nchunks_ - 1], 0) == cudaSuccess;
+    if (!ok) return st ? st : GEXS_ERR_CUDA;
+    return st;
 }
 
 void B200Manager::TransferResults(double* h_freq, double* h_intens, int N)
@@ -174,6 +332,7 @@ void B200Manager::TransferResults(double* h_freq, double* h_intens, int N, int I
 void B200Manager::Cleanup()
 {
     if (ctx_) { flush(); cudaStreamSynchronize((cudaStream_t)stream_); }
+    if (copy_stream_) cudaStreamSynchronize((cudaStream_t)copy_stream_);
     cudaSetDevice(device_);
     for (double* d : d_slots_) cudaFree(d);
     d_slots_.clear();

@@ -19,6 +19,19 @@
  * TransferVectors, TransferResults, ReadyForWork or Cleanup).  Errors are
  * kept in last_status() instead of exit(-1).  The lines of a chunk must be
  * sorted by nu, as BaseProfile streams them.
+ *
+ * Overlapped transfer (lists of 2^21 lines or more): TransferVectors
+ * copies the lines in 32 pieces on a copy stream, one event per piece, and
+ * keeps every (N/8192)-th nu.  The first launch after it runs each queued
+ * pair as grid segments cut at the line quantiles 1/32, 1/8, 1/4, 1/2
+ * (each segment starting at a multiple of 4096 bins, the widest tile, from
+ * the pair's start_idx, so the tiles are those of one launch); a segment
+ * sees only the lines that can reach it and waits only for the pieces
+ * holding them, and each segment has a compute stream of its own, so that
+ * the long tiles of dense spectral regions start as soon as their lines
+ * have arrived while later segments fill the free SMs.  The sums are bit-for-bit those of a single launch.
+ * Host buffers must stay valid until TransferResults (or Cleanup), as with
+ * any asynchronous copy; pageable buffers work but do not overlap.
  */
 #pragma once
 #include <cstddef>
@@ -63,12 +76,22 @@ public:
 
 private:
     int flush();
+    int run_segmented();
     int fail(int st);
+    size_t lines_below(double v) const;
+    size_t lines_upto(double v) const;
+    double nu_at(size_t i) const;
 
     int device_, convention_, precision_;
     size_t memory_bytes_;
     gexs_ctx* ctx_ = nullptr;
     void* stream_ = nullptr;
+    std::vector<void*> seg_stream_;  /* one compute stream per further segment */
+    void* copy_stream_ = nullptr;    /* line pieces host -> device */
+    std::vector<void*> chunk_ev_;    /* piece c of the lines has arrived */
+    void* done_ev_ = nullptr;        /* queued kernels are done with the lines */
+    void* fork_ev_ = nullptr;
+    std::vector<void*> join_ev_;     /* segment stream s has finished */
     int status_ = GEXS_OK;
 
     int npoints_ = 0;
@@ -78,6 +101,12 @@ private:
     int* d_g_ = nullptr;
     size_t nlines_ = 0;
     int tasks_ = 0;
+    /* overlapped transfer state */
+    int nchunks_ = 0;
+    size_t chunk_lines_ = 0;
+    bool fresh_ = false;             /* pieces not yet all awaited by stream_ */
+    std::vector<size_t> samp_idx_;   /* sampled line indices (ascending, last = N-1) */
+    std::vector<double> samp_nu_;    /* nu at those indices */
 
     double half_width_ = 0, temperature_ = 0, partition_ = 0, dfreq_ = 0, mass_ = 0;
     double pressure_ = 0, ref_temp_ = 296.0, ref_press_ = 1.0;

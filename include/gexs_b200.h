@@ -160,6 +160,12 @@ typedef struct gexs_launch_cfg {
  * once per job by a prep kernel (no per-job scratch of 24 B per line) */
 #define GEXS_LAUNCH_DERIVE_ON_LOAD 1
 
+/* A context owns a stream-ordered memory pool on its device for the
+ * launch tables and per-line prep arrays (24 B per line) of gexs_run.  The
+ * pool keeps its memory between calls (no remapping per call) and never
+ * makes an allocation on one stream wait for a free on another, so
+ * gexs_run calls on different streams overlap; its memory goes back to the
+ * device at gexs_ctx_destroy. */
 int         gexs_ctx_create(int device, gexs_ctx** out);
 int         gexs_ctx_destroy(gexs_ctx* ctx);
 const char* gexs_status_string(int status);
