@@ -85,3 +85,57 @@ def test_overlapped_transfer_is_bitwise_one_launch(conv, precision, hw):
     T, P, s0, npts, ne = pairs[0]
     want2 = _reference(ctx, L2, seeds, conv, precision, hw, T, P, qs[0], s0, npts, ne)
     assert np.array_equal(o2.view(np.int64), want2.view(np.int64))
+
+
+def test_overlapped_pairs_queued_together_and_doppler():
+    """Three Voigt pairs queued before the first TransferResults (one
+    segmented flush with three jobs per segment launch), then a Doppler
+    manager on the same list without gamma and n."""
+    n = 2_500_000
+    L, h = _lines(n, 909)
+    freq = NU0 + np.arange(NPTS, dtype=np.float64) * DNU
+    seeds = np.zeros(NPTS)
+    pairs = [(1500.0, 1.0, 0, NPTS, n), (300.0, 5.0, 4097, NPTS - 9000, n - 5),
+             (2500.0, 0.01, 77777, 300000, n)]
+    qs = [1000.0, 250.0, 3000.0]
+    m = Manager(capi.VOIGT, 0, capi.CONV_PHYSICAL, capi.FP32,
+                memory_bytes=(n * 44) + 4 * NPTS * 8 + (64 << 20))
+    m.initialize_vectors(NPTS, 3)
+    m.transfer_freq(freq, seeds)
+    m.initialize_constants(0.0, 296.0, qs[0], DNU, MASS, 1.0, REF_T, REF_P)
+    m.transfer_vectors(h["elow"].numpy(), h["nu"].numpy(), h["aif"].numpy(), h["gns"].numpy(),
+                       h["gamma"].numpy(), h["n"].numpy())
+    for (T, P, s0, npts, ne), q in zip(pairs, qs):
+        m.execute(npts, ne, s0, T, P, q)
+    got = []
+    for i in range(3):
+        o = np.zeros(NPTS)
+        m.transfer_results(np.zeros(NPTS), o, i)
+        got.append(o)
+    m.close()
+    ctx = Context(0)
+    for (T, P, s0, npts, ne), q, o in zip(pairs, qs, got):
+        want = _reference(ctx, L, seeds, capi.CONV_PHYSICAL, capi.FP32, 0.0, T, P, q, s0, npts, ne)
+        assert np.any(o != 0.0)
+        assert np.array_equal(o.view(np.int64), want.view(np.int64))
+
+    d = Manager(capi.DOPPLER, 0, capi.CONV_PHYSICAL, capi.FP32,
+                memory_bytes=(n * 28) + 2 * NPTS * 8 + (64 << 20))
+    d.initialize_vectors(NPTS, 1)
+    d.transfer_freq(freq, seeds)
+    d.initialize_constants(0.0, 296.0, qs[0], DNU, MASS, 1.0, REF_T, REF_P)
+    d.transfer_vectors(h["elow"].numpy(), h["nu"].numpy(), h["aif"].numpy(), h["gns"].numpy())
+    d.execute(NPTS, n, 0, 1200.0, 1.0, qs[0])
+    o = np.zeros(NPTS)
+    d.transfer_results(np.zeros(NPTS), o, 0)
+    d.close()
+    lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"])
+    out = torch.zeros(NPTS, dtype=torch.float64, device="cuda")
+    j = Job(lines, out, convention=capi.CONV_PHYSICAL, profile=capi.DOPPLER, temperature=1200.0,
+            pressure=1.0, partition=qs[0], mass=MASS, nu_start=NU0, dnu=DNU, grid_points=NPTS,
+            precision=capi.FP32, ref_temp=REF_T, ref_press=REF_P, accumulate=1)
+    ctx.run([j])
+    ctx.check()
+    want = out.cpu().numpy()
+    assert np.any(o != 0.0)
+    assert np.array_equal(o.view(np.int64), want.view(np.int64))
