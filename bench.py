@@ -17,7 +17,10 @@ e2e    = the same through the drop-in manager's C ABI (gexs_manager_*):
 also   = plain FP64 per-(T,P) GPU path on the same workload, the 64-pair
          uneven-grid batch (FP32, one persistent launch replayed from a CUDA
          graph) against the plain FP64 path pair by pair, roofline, the
-         reference's own CPU path timed on a bounded sample.
+         reference's own CPU path timed on a bounded sample, and the
+         reference's own GPU kernel (built for sm_100a) on a bounded sample
+         of the same list against ours on the same lines and bins
+         (--no-cpu skips both reference legs).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
@@ -104,6 +107,63 @@ def device_id_for_smi(torch, dev):
 
 
 # --------------------------------------------------------- CPU baseline
+def gpu_reference_sample(torch, ctx, L, q, dev, k=1_000_000, reps=3):
+    """The reference's own GPU path on this B200: GpuManager with the v2 Voigt
+    kernel (Managers/Accel/GPU/GPUManager.cpp, compute/CUDA/cross_kernal_v2.cu
+    :403-457, one CTA per bin scanning the list), built for sm_100a as
+    oracle/_ref/gexsref_gpu, on k consecutive lines around the median nu0 of
+    the workload's own list, over the bins within its 100 cm^-1 window.  The
+    same lines and grid run through our reference-GPU convention (inclusive
+    100 cm^-1 window, the same (line, bin) pairs, counted exactly) in the
+    FP32 form; the FP64 form gives the agreement.  A bounded sample: the
+    reference kernel's scan grows with lines x bins, so the full list would
+    take minutes per pair."""
+    from gexs_b200 import Job, LineList, _capi as capi
+    from oracle import pyoracle as po
+    if not po.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/gexsref_gpu not built"}
+    n = int(L["nu"].shape[0])
+    a = max(0, n // 2 - k // 2)
+    b = min(n, a + k)
+    S = {kk: v[a:b].cpu().numpy() for kk, v in L.items()}
+    lo = float(S["nu"][0]) - 100.0 - 1.0
+    nb = int((float(S["nu"][-1]) + 100.0 + 1.0 - lo) / DNU) + 1
+    budget = (b - a) * 52 + nb * 16 + (64 << 20)
+    sig, ms = po.ref_gpu_voigt(S, lo, DNU, nb, T_K, P_BAR, q, MASS, 296.0, 1.0, 0.0,
+                               reps=reps, budget_bytes=budget)
+    ref_ms = min(ms[1:]) if len(ms) > 1 else ms[0]
+    lines = LineList(*[L[kk][a:b] for kk in ("nu", "elow", "aif", "gns", "gamma", "n")])
+    res = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for prec, name in ((capi.FP32, "fp32"), (capi.FP64, "fp64")):
+        out = torch.zeros(nb, dtype=torch.float64, device=dev)
+        j = Job(lines, out, convention=capi.CONV_REF_GPU, profile=capi.VOIGT, temperature=T_K,
+                pressure=P_BAR, partition=q, mass=MASS, nu_start=lo, dnu=DNU, grid_points=nb,
+                precision=prec, ref_temp=296.0, ref_press=1.0)
+        ctx.run([j])
+        ctx.check()
+        ts = []
+        for _ in range(3):
+            e0.record(); ctx.run([j]); e1.record(); e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        o = out.cpu().numpy()
+        m = o > 1e-6 * o.max()
+        res[name] = {"ms": min(ts),
+                     "max_rel_vs_reference": float(np.max(np.abs(sig[m] - o[m]) / o[m]))}
+        if prec == capi.FP64:
+            evals = ctx.count_evals([j])[0]
+    return {"sample": "%d consecutive lines around the median nu0 of the workload's list, "
+                      "%d bins (its 100 cm^-1 window), reference-GPU convention" % (b - a, nb),
+            "evals": evals, "reference_ms": ref_ms, "reference_evals_per_s": evals / (ref_ms * 1e-3),
+            "ours_fp32_ms": res["fp32"]["ms"], "ours_fp32_evals_per_s": evals / (res["fp32"]["ms"] * 1e-3),
+            "ours_fp64_ms": res["fp64"]["ms"],
+            "speedup_fp32": ref_ms / res["fp32"]["ms"], "speedup_fp64": ref_ms / res["fp64"]["ms"],
+            "max_rel_fp64_vs_reference": res["fp64"]["max_rel_vs_reference"],
+            "max_rel_fp32_vs_reference": res["fp32"]["max_rel_vs_reference"],
+            "reference_build": "reference sources compiled for sm_100a; __shfl_xor mapped to "
+                               "__shfl_xor_sync (oracle/ref_gpu_shim.h), nothing else changed"}
+
+
 def cpu_reference_sample(target_s=12.0, seed_states=1002, seed_lines=2002):
     """Reference CPU path (OpenMPManager::ComputeVoigtTP + humlic, compiled
     from the reference sources at -O3 -march=x86-64-v3) on a bounded sample
@@ -678,6 +738,8 @@ def our_arm(args):
                          "fp32_band_rel_vs_fp64": band_err, "integrated_fp64": integral},
             "clocks": clocks,
         }
+    if not args.no_cpu and rank == 0 and ws == 1:
+        result["reference_gpu_kernel"] = gpu_reference_sample(torch, ctx, L, q, dev)
     if not args.no_batch and rank == 0:
         result["batch64"] = batch64(ctx, torch, dev)
     if not args.no_serve and rank == 0:
@@ -704,7 +766,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lines", type=int, default=100_000_000)
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the reference legs (CPU sample, reference GPU kernel)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest"],
                     help="quad: Gauss-Hermite 16/32 vs Humlicek on the 5e8-line list; "

@@ -13,6 +13,7 @@ ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgexsref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libgexsref_fast.so")
 REF_READER_BIN = os.path.join(HERE, "_ref", "gexsref_reader")
+REF_GPU_BIN = os.path.join(HERE, "_ref", "gexsref_gpu")
 
 _orc = None
 _refs = {}
@@ -257,3 +258,38 @@ def ref_hitran_read(path, pressure=1.0, mixture=1.0, ref_q=1.0):
     arr = raw[8:].view(np.float64).reshape(6, n) if n else np.zeros((6, 0))
     keys = ("nu", "gns", "elow", "aif", "gamma", "n")
     return {k: arr[i].copy() for i, k in enumerate(keys)}
+
+
+def ref_gpu_available():
+    return os.path.exists(REF_GPU_BIN)
+
+
+def ref_gpu_voigt(lines, nu_start, dnu, npts, temperature, pressure, partition, mass,
+                  ref_temp=296.0, ref_press=1.0, half_width=0.0, reps=1,
+                  budget_bytes=1 << 30, timeout=600):
+    """The reference's GPU manager and v2 Voigt kernel (GpuManager,
+    compute/CUDA/cross_kernal_v2.cu:403-457, built for sm_100a as
+    oracle/_ref/gexsref_gpu) on one (T, P) pair over the grid nu_start +
+    j*dnu, j < npts: returns (sigma, [ms per repetition]).  Needs a GPU; the
+    reference window is its LORENTZ_CUTOFF (100 cm^-1, inclusive)."""
+    import json
+    import subprocess
+    import tempfile
+    n = int(len(lines["nu"]))
+    hdr = np.array([n, int(npts), int(reps), int(budget_bytes)], dtype=np.int64)
+    par = np.array([nu_start, dnu, temperature, pressure, partition, mass, ref_temp, ref_press,
+                    half_width], dtype=np.float64)
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(inp, "wb") as f:
+            f.write(hdr.tobytes()); f.write(par.tobytes())
+            for k in ("elow", "nu", "aif"):
+                f.write(np.ascontiguousarray(lines[k], dtype=np.float64).tobytes())
+            f.write(np.ascontiguousarray(lines["gns"], dtype=np.int32).tobytes())
+            for k in ("gamma", "n"):
+                f.write(np.ascontiguousarray(lines[k], dtype=np.float64).tobytes())
+        p = subprocess.run([REF_GPU_BIN, inp, out], check=True, capture_output=True, text=True,
+                           timeout=timeout)
+        sigma = np.fromfile(out, dtype=np.float64)
+    ms = json.loads(p.stdout.strip().splitlines()[-1])["ms"]
+    return sigma, ms
