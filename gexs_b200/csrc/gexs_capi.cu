@@ -159,9 +159,15 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
 struct Layout {
     size_t op, oc, opp, oprep, bytes;
     std::vector<size_t> job_prep;   /* byte offset of each job's prep arrays */
+    /* line-slice tables (FP32 Voigt groups): offsets, item bound, lines per slice */
+    bool sliced = false;
+    size_t os_prefix = 0, os_counts = 0, os_rowbase = 0, os_ticket = 0, os_lohi = 0, os_nitems = 0,
+           os_rows = 0;
+    int max_rows = 0;
+    long long lines_per_slice = 0;
 };
 
-static Layout group_layout(const Group& g, bool prep)
+static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg)
 {
     Layout L;
     auto up = [](size_t a) { return (a + 255) & ~size_t(255); };
@@ -176,6 +182,19 @@ static Layout group_layout(const Group& g, bool prep)
     for (const gexs_job& j : g.jobs) {
         L.job_prep.push_back(a);
         if (prep) a = up(a + (size_t)j.lines.count * 3 * sizeof(double));
+    }
+    if (slices_apply(g.pk, g.prec) && g.nitems > 0) {
+        const int W = tile_bins(cfg);
+        const size_t nt = (size_t)g.nitems;
+        L.sliced = true;
+        L.lines_per_slice = slice_lines(g.jobs.data(), (int)g.jobs.size(), W, &L.max_rows);
+        L.os_prefix = up(a); a = L.os_prefix + (nt + 1) * sizeof(int);
+        L.os_counts = up(a); a = L.os_counts + nt * sizeof(int);
+        L.os_rowbase = up(a); a = L.os_rowbase + nt * sizeof(int);
+        L.os_ticket = up(a); a = L.os_ticket + nt * sizeof(int);
+        L.os_lohi = up(a);   a = L.os_lohi + 2 * nt * sizeof(long long);
+        L.os_nitems = up(a); a = L.os_nitems + 256;
+        L.os_rows = up(a);   a = L.os_rows + (size_t)L.max_rows * W * sizeof(double);
     }
     L.bytes = a + 256;
     return L;
@@ -208,9 +227,22 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
     cudaError_t e = cudaSuccess;
     if (prep) e = launch_prep((const gexs_job*)d, pp, (int)g.jobs.size(), max_lines(g), nsm, s);
     if (e != cudaSuccess) return e;
+    SliceTables sl;
+    std::memset(&sl, 0, sizeof(sl));
+    if (L.sliced) {
+        sl.prefix = (int*)(d + L.os_prefix);
+        sl.counts = (int*)(d + L.os_counts);
+        sl.rowbase = (int*)(d + L.os_rowbase);
+        sl.ticket = (int*)(d + L.os_ticket);
+        sl.lohi = (long long*)(d + L.os_lohi);
+        sl.nitems = (int*)(d + L.os_nitems);
+        sl.rows = (double*)(d + L.os_rows);
+        sl.max_rows = L.max_rows;
+        sl.lines_per_slice = L.lines_per_slice;
+    }
     return launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + L.op),
                         (int)g.jobs.size(), g.nitems, (int*)(d + L.oc), d_err,
-                        prep ? pp : nullptr, cfg, nsm, s);
+                        prep ? pp : nullptr, cfg, nsm, s, L.sliced ? &sl : nullptr);
 }
 
 extern "C" {
@@ -381,7 +413,7 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
         const Group& g = groups[gi];
         if (g.nitems == 0) continue;
         const bool prep = !(cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
-        Layout L = group_layout(g, prep);
+        Layout L = group_layout(g, prep, cfgs[gi]);
         void* d = nullptr;
         e = ctx->pool ? cudaMallocFromPoolAsync(&d, L.bytes, ctx->pool, s)
                       : cudaMallocAsync(&d, L.bytes, s);
@@ -465,7 +497,7 @@ int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const Group& g = b->groups[gi];
         const bool prep = !(b->cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
-        Layout L = group_layout(g, prep);
+        Layout L = group_layout(g, prep, b->cfgs[gi]);
         void* d = nullptr;
         if (cudaMalloc(&d, L.bytes) != cudaSuccess) { gexs_batch_destroy(b); return set_error(GEXS_ERR_OOM, "batch tables"); }
         b->dmem.push_back(d); b->layouts.push_back(L); b->prep.push_back(prep);

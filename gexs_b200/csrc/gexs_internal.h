@@ -10,6 +10,25 @@ namespace gexs {
 /* kernel launchers (gexs_kernels.cu; tile kernels in gexs_tiles.cuh) */
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
+/* Line slices of the FP32 Voigt region-I kernel: a tile whose line range
+ * holds more than `lines_per_slice` lines is cut into ceil(n / lines_per_
+ * slice) work items (the count depends on the tile alone, so the same tile
+ * is cut the same way in every launch).  A split tile's slices write
+ * partial rows; the last one to finish sums them in slice order into the
+ * output.  All arrays live in the launch table; slice_plan_kernel fills
+ * them (and zeroes the tickets) before the region-I kernel runs. */
+struct SliceTables {
+    int*       prefix;      /* ntiles + 1: first item of each tile       */
+    int*       counts;      /* ntiles: slices per tile                   */
+    int*       rowbase;     /* ntiles: first partial row of a split tile */
+    int*       ticket;      /* ntiles: slices finished                   */
+    long long* lohi;        /* 2 ntiles: each tile's line range          */
+    int*       nitems;      /* 1: items of the launch                    */
+    double*    rows;        /* max_rows x tile bins: partial rows        */
+    int        max_rows;
+    long long  lines_per_slice;
+};
+
 /* d_prep: device array of per-job prep arrays (S | invw | y, 3 N doubles
  * each, from launch_prep), or NULL to derive every line on load.
  * d_counter: a 256-byte block of work counters; the caller zeroes the
@@ -18,7 +37,12 @@ int tile_bins(const gexs_launch_cfg& c);
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st);
+                         cudaStream_t st, const SliceTables* sl = nullptr);
+/* FP32 Voigt groups are sliced; lines_per_slice for a group (grows only
+ * when the partial rows of its split tiles could pass 1 GiB) and the bound
+ * on those rows */
+bool slices_apply(int pk, int prec);
+long long slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows);
 cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs,
                         int64_t max_lines, int nsm, cudaStream_t st);
 cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,

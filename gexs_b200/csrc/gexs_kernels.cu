@@ -3,7 +3,9 @@
  * Q(T), and the front of the tile-kernel dispatch (the tile kernel itself
  * is in gexs_tiles.cuh).
  */
+#include <cmath>
 #include <cstring>
+#include <cub/cub.cuh>
 #include "gexs_tiles.cuh"
 
 namespace gexs {
@@ -112,12 +114,14 @@ int profile_class(const gexs_job& j)
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st)
+                         cudaStream_t st, const SliceTables* sl)
 {
     KArgs a;
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
     a.counter = d_counter; a.err = d_err; a.prep = d_prep;
     a.tile_w = tile_bins(cfg);
+    std::memset(&a.sl, 0, sizeof(a.sl));
+    if (sl && slices_apply(pk, prec)) a.sl = *sl;
     switch (pk) {
     case PK_VOIGT: return launch_tiles_voigt(prec, a, cfg, nsm, st);
     case PK_ERF:   return launch_tiles_erf(prec, a, cfg, nsm, st);
@@ -138,6 +142,111 @@ cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs
 }
 
 int tile_bins(const gexs_launch_cfg& c) { return 32 * c.bins_per_lane * c.warps; }
+
+/* ------------------------------------------------------------ line slices */
+namespace {
+/* one warp per tile: the tile's line range, searched exactly as the
+ * region-I kernel's producers search it, and its slice count */
+__global__ void slice_plan_kernel(const KArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ti >= a.nitems) return;
+    int jl = 0, jh = a.njobs;
+    while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
+    const gexs_job& J = a.jobs[jl];
+    const int64_t j0 = J.start_idx + (int64_t)(ti - __ldg(a.prefix + jl)) * a.tile_w;
+    const int jn = (int)min((int64_t)a.tile_w, J.start_idx + J.n_points - j0);
+    const double f0 = grid_f(J.nu_start, J.dnu, j0);
+    const double fl = grid_f(J.nu_start, J.dnu, j0 + jn - 1);
+    const int64_t nl = J.lines.count;
+    const double margin = 2.0 * J.dnu + 1e-9 * (fabs(fl) + J.cutoff);
+    const int64_t lo = warp_bound<false>(J.lines.nu, nl, f0 - J.cutoff - margin, lane);
+    const int64_t hi = max(warp_bound<true>(J.lines.nu, nl, fl + J.cutoff + margin, lane), lo);
+    if (lane == 0) {
+        const long long n = hi - lo, per = a.sl.lines_per_slice;
+        a.sl.lohi[2 * ti] = lo;
+        a.sl.lohi[2 * ti + 1] = hi;
+        a.sl.counts[ti] = n > per ? (int)((n + per - 1) / per) : 1;
+        a.sl.ticket[ti] = 0;
+    }
+}
+
+/* one CTA: exclusive prefixes of the slice counts (items) and of the
+ * slices of split tiles (partial rows), and the item count */
+__global__ void __launch_bounds__(1024) slice_scan_kernel(const KArgs a)
+{
+    typedef cub::BlockScan<int, 1024> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ long long carry, rcarry;
+    if (threadIdx.x == 0) { carry = 0; rcarry = 0; }
+    __syncthreads();
+    for (int base = 0; base < a.nitems; base += 1024) {
+        const int i = base + (int)threadIdx.x;
+        const int v = i < a.nitems ? a.sl.counts[i] : 0;
+        const int r = v > 1 ? v : 0;
+        int ex = 0, tot = 0, rex = 0, rtot = 0;
+        Scan(tmp).ExclusiveSum(v, ex, tot);
+        __syncthreads();
+        Scan(tmp).ExclusiveSum(r, rex, rtot);
+        if (i < a.nitems) {
+            a.sl.prefix[i] = (int)min(carry + ex, (long long)INT32_MAX);
+            a.sl.rowbase[i] = (int)min(rcarry + rex, (long long)INT32_MAX);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { carry += tot; rcarry += rtot; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (rcarry > a.sl.max_rows || carry > INT32_MAX) {
+            /* cannot happen with the host's bound; run no item rather than
+             * write past the partial rows */
+            atomicOr(a.err, GEXS_KERR_SLICES);
+            *a.sl.nitems = 0;
+        } else {
+            a.sl.prefix[a.nitems] = (int)carry;
+            *a.sl.nitems = (int)carry;
+        }
+    }
+}
+}  // namespace
+
+cudaError_t launch_slice_plan(const KArgs& a, cudaStream_t st)
+{
+    if (a.nitems <= 0) return cudaSuccess;
+    slice_plan_kernel<<<(a.nitems + 7) / 8, 256, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    slice_scan_kernel<<<1, 1024, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+bool slices_apply(int pk, int prec) { return pk == PK_VOIGT && prec == GEXS_FP32; }
+
+long long slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows)
+{
+    /* A line lies in at most (2 (cutoff + margin)) / (tile width) + 2 tiles,
+     * so the tiles hold at most sum(lines x that) = M line entries.  A split
+     * tile (n > per lines) has ceil(n / per) < 2 n / per slices, so the
+     * slices of split tiles, which alone need partial rows, are fewer than
+     * 2 M / per.  per doubles until those rows fit in 1 GiB; past 2^40 no
+     * tile can be split at all. */
+    long long per = 65536;
+    for (;;) {
+        double rows = 0.0;
+        for (int i = 0; i < njobs; ++i) {
+            const gexs_job& j = jobs[i];
+            const double tpl = std::floor((2.0 * j.cutoff + 8.0 * j.dnu) / ((double)tile_w * j.dnu)) + 3.0;
+            rows += 2.0 * std::ceil((double)j.lines.count * tpl / (double)per);
+        }
+        if (rows * tile_w * sizeof(double) <= (double)(1ull << 30)) {
+            *max_rows = (int)rows;
+            return per;
+        }
+        if (per >= (1ll << 40)) { *max_rows = 0; return 1ll << 62; }
+        per *= 2;
+    }
+}
 
 /* ----------------------------------------------- control writes as kernels */
 namespace {

@@ -310,7 +310,12 @@ struct KArgs {
     int*            err;       /* sticky error word                      */
     double* const*  prep;      /* per job S|invw|y arrays, or NULL       */
     int             tile_w;    /* bins per work item (core kernel)       */
+    SliceTables     sl;        /* line slices (sl.prefix NULL: none)     */
 };
+
+/* slice_plan_kernel + slice_scan_kernel (gexs_kernels.cu): every tile's
+ * line range and slice count, then the item prefix and count */
+cudaError_t launch_slice_plan(const KArgs& a, cudaStream_t st);
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
 {
@@ -933,14 +938,16 @@ constexpr int WS_STAGES = 4;
 constexpr int WS_R = 128;
 constexpr int WS_SPIN = 1 << 21;          /* try_wait attempts before giving up */
 constexpr int GEXS_KERR_PIPELINE = 1;
+constexpr int GEXS_KERR_SLICES = 2;     /* more line slices than the tables hold */
 
 struct StageHdr {
     long long j0;          /* absolute first bin of the tile                */
     int jl;                /* job index                                     */
     int jn;                /* bins in the tile                              */
     int nrec;              /* records in this stage                         */
-    int flags;             /* 1 first stage of the tile, 2 last, 4 end      */
-    int pad0, pad1;
+    int flags;             /* 1 first stage of the tile, 2 last, 4 end,
+                              8 the item is one slice of a split tile       */
+    int item, tile;        /* work item and its tile                        */
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
@@ -983,7 +990,8 @@ struct WsSmem {
     static constexpr size_t off_rec = 0;
     static constexpr size_t off_hdr = off_rec + (size_t)WS_STAGES * WS_R * sizeof(RecV);
     static constexpr size_t off_bar = off_hdr + (size_t)WS_STAGES * sizeof(StageHdr);
-    /* mbarriers: full[WS_STAGES], empty[WS_STAGES], producers' own barrier */
+    /* mbarriers: full[WS_STAGES], empty[WS_STAGES], producers' own barrier,
+     * consumers' own barrier */
     static constexpr size_t off_stg = off_bar + (size_t)(2 * WS_STAGES + 2) * sizeof(unsigned long long);
     static constexpr size_t off_gn = off_stg + (size_t)NF64 * 2 * NP * sizeof(double);
     static constexpr size_t off_kahan = (off_gn + (PREP ? 0 : (size_t)2 * NP * sizeof(int)) + 15) & ~size_t(15);
@@ -1012,9 +1020,12 @@ voigt_ws_kernel(const KArgs args)
     __shared__ long long s_lohi[2];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool sliced = args.sl.prefix != nullptr;
+    const int nitems = sliced ? *(volatile const int*)args.sl.nitems : args.nitems;
     if (tid == 0) {
         for (int st = 0; st < WS_STAGES; ++st) { mbar_init(s_full + st, NP); mbar_init(s_empty + st, CONS); }
         mbar_init(s_pbar, NP);
+        mbar_init(s_pbar + 1, CONS);
     }
     __syncthreads();   /* the only CTA-wide barrier: before the roles split */
 
@@ -1040,32 +1051,52 @@ voigt_ws_kernel(const KArgs args)
             if (ptid == 0) s_item = atomicAdd(args.counter, 1);
             if (!psync()) { fail(); return; }
             const int item = s_item;
-            if (item >= args.nitems) {
+            if (item >= nitems) {
                 if (!mbar_wait(s_empty + st, ph)) { fail(); return; }
                 if (ptid == 0) { s_hdr[st].flags = 4; s_hdr[st].nrec = 0; }
                 mbar_arrive(s_full + st);
                 return;
             }
+            /* item -> (tile, slice): one item per tile unless sliced */
+            int ti = item, sidx = 0, ns = 1;
+            if (sliced) {
+                int tl = 0, th = args.nitems;
+                while (th - tl > 1) { int m = (tl + th) >> 1; if (__ldg(args.sl.prefix + m) <= item) tl = m; else th = m; }
+                ti = tl;
+                sidx = item - __ldg(args.sl.prefix + tl);
+                ns = __ldg(args.sl.prefix + tl + 1) - __ldg(args.sl.prefix + tl);
+            }
             int jl = 0, jh = args.njobs;
-            while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= item) jl = m; else jh = m; }
+            while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
             const gexs_job* Jp = args.jobs + jl;
             const gexs_job& J = *Jp;
             Tile T;
             T.J = Jp;
-            T.j0 = J.start_idx + (int64_t)(item - __ldg(args.prefix + jl)) * W;
+            T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * W;
             T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
             T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
             T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
             T.inv_dnu = 1.0 / J.dnu;
             const int64_t nl = J.lines.count;
             const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
-            if (pw == 0) {
-                int64_t v = warp_bound<false>(J.lines.nu, nl, T.f0 - J.cutoff - margin, lane);
-                if (lane == 0) s_lohi[0] = v;
-            }
-            if (pw == (PROD > 1 ? 1 : 0)) {
-                int64_t v = warp_bound<true>(J.lines.nu, nl, T.fl + J.cutoff + margin, lane);
-                if (lane == 0) s_lohi[1] = v;
+            if (sliced) {
+                /* the tile's range from slice_plan_kernel, cut into ns equal parts */
+                if (ptid == 0) {
+                    const long long tlo = __ldg(args.sl.lohi + 2 * ti), thi = __ldg(args.sl.lohi + 2 * ti + 1);
+                    const long long per = (thi - tlo + ns - 1) / ns;
+                    const long long a0 = tlo + (long long)sidx * per;
+                    s_lohi[0] = min(a0, thi);
+                    s_lohi[1] = min(a0 + per, thi);
+                }
+            } else {
+                if (pw == 0) {
+                    int64_t v = warp_bound<false>(J.lines.nu, nl, T.f0 - J.cutoff - margin, lane);
+                    if (lane == 0) s_lohi[0] = v;
+                }
+                if (pw == (PROD > 1 ? 1 : 0)) {
+                    int64_t v = warp_bound<true>(J.lines.nu, nl, T.fl + J.cutoff + margin, lane);
+                    if (lane == 0) s_lohi[1] = v;
+                }
             }
             if (!psync()) { fail(); return; }
             const int64_t lo = s_lohi[0];
@@ -1130,8 +1161,9 @@ voigt_ws_kernel(const KArgs args)
                 if (ptid == 0) {
                     StageHdr h;
                     h.j0 = T.j0; h.jl = jl; h.jn = T.jn; h.nrec = nrec;
-                    h.flags = (c == 0 ? 1 : 0) | (c == nchunk - 1 ? 2 : 0);
-                    h.pad0 = h.pad1 = 0;
+                    h.flags = (c == 0 ? 1 : 0) | (c == nchunk - 1 ? 2 : 0) | (ns > 1 ? 8 : 0);
+                    h.item = item;
+                    h.tile = ti;
                     s_hdr[st] = h;
                 }
                 mbar_arrive(s_full + st);
@@ -1146,6 +1178,16 @@ voigt_ws_kernel(const KArgs args)
     /* ---------------------------------------------------------- consumers */
     int st = 0;
     unsigned ph = 0;
+    /* barrier among the consumer warps (a split tile's merge), bounded */
+    unsigned cph = 0;
+    __shared__ int s_last;
+    auto csync = [&]() -> bool {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(s_pbar + 1);
+        const bool ok = mbar_wait(s_pbar + 1, cph);
+        cph ^= 1;
+        return ok;
+    };
     float2 part[B / 2];
 #pragma unroll
     for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
@@ -1171,7 +1213,7 @@ voigt_ws_kernel(const KArgs args)
         }
 #pragma unroll
         for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
-        if (h.flags & 2) {
+        if ((h.flags & 2) && !(h.flags & 8)) {
             const gexs_job& J = args.jobs[h.jl];
             double* out = J.out;
 #pragma unroll
@@ -1181,6 +1223,37 @@ voigt_ws_kernel(const KArgs args)
                     const double v = (double)s_ks[t] - (double)s_kc[t];
                     const int64_t j = h.j0 + t;
                     out[j] = J.accumulate ? out[j] + v : v;
+                }
+            }
+        } else if (h.flags & 2) {
+            /* one slice of a split tile: its partial row, then a ticket; the
+             * last slice to finish adds the rows in slice order */
+            const gexs_job& J = args.jobs[h.jl];
+            double* out = J.out;
+            const int base = args.sl.prefix[h.tile];
+            const int ns = args.sl.prefix[h.tile + 1] - base;
+            const int rb = args.sl.rowbase[h.tile];
+            double* row = args.sl.rows + (size_t)(rb + (h.item - base)) * W;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = warp * 32 * B + lane + 32 * k;
+                if (t < h.jn) row[t] = (double)s_ks[t] - (double)s_kc[t];
+            }
+            __threadfence();
+            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+            if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile, 1) == ns - 1;
+            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+            if (s_last) {
+                __threadfence();
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    if (t < h.jn) {
+                        double v = 0.0;
+                        for (int q = 0; q < ns; ++q) v += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
+                        const int64_t j = h.j0 + t;
+                        out[j] = J.accumulate ? out[j] + v : v;
+                    }
                 }
             }
         }
@@ -1388,7 +1461,8 @@ static cudaError_t launch_ws_one(const KArgs& a, int ctas_per_sm, int nsm, cudaS
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     const int per = ctas_per_sm > 0 ? min(ctas_per_sm, occ) : occ;
-    const int grid = max(1, min(a.nitems, per * nsm));
+    /* sliced: the item count is known on the device only */
+    const int grid = a.sl.prefix ? per * nsm : max(1, min(a.nitems, per * nsm));
     kern<<<grid, (CONS + PROD) * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
@@ -1419,6 +1493,10 @@ template <int PK, int PREC, bool PREP>
 static cudaError_t launch_cfg(const KArgs& a, const gexs_launch_cfg& c, int nsm, cudaStream_t st)
 {
     if constexpr (PK == PK_VOIGT && PREC == GEXS_FP32) {
+        if (a.sl.prefix) {
+            cudaError_t e = launch_slice_plan(a, st);
+            if (e != cudaSuccess) return e;
+        }
         return launch_ws<PREP>(a, c, nsm, st);
     } else {
         if (c.bins_per_lane == 16) {
