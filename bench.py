@@ -713,9 +713,10 @@ def our_arm(args):
                        "l2": "inputs (%.1f GB of lines) larger than L2" % (line_bytes / 1e9),
                        "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]}},
             # per step: put_blob_kernel (launch table), prep_kernel (S(T),
-            # width, y per line), voigt_ws_kernel (region I), zero_ints_kernel
+            # width, y per line), slice_plan_kernel and slice_scan_kernel
+            # (line slices), voigt_ws_kernel (region I), zero_ints_kernel
             # (core work counter) and core_kernel (Humlicek regions II-IV)
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": 7 * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": traffic,

@@ -10,7 +10,8 @@ namespace gexs {
 /* kernel launchers (gexs_kernels.cu; tile kernels in gexs_tiles.cuh) */
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
-/* Line slices of the FP32 Voigt region-I kernel: a tile whose line range
+/* Line slices of the tile kernels (the FP32 Voigt region-I kernel and
+ * tile_kernel; not the FP32 Voigt core kernel): a tile whose line range
  * holds more than `lines_per_slice` lines is cut into ceil(n / lines_per_
  * slice) work items (the count depends on the tile alone, so the same tile
  * is cut the same way in every launch).  A split tile's slices write
@@ -38,7 +39,7 @@ cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
                          cudaStream_t st, const SliceTables* sl = nullptr);
-/* FP32 Voigt groups are sliced; lines_per_slice for a group (grows only
+/* which groups are sliced (all); lines_per_slice for a group (grows only
  * when the partial rows of its split tiles could pass 1 GiB) and the bound
  * on those rows */
 bool slices_apply(int pk, int prec);

@@ -221,7 +221,7 @@ cudaError_t launch_slice_plan(const KArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-bool slices_apply(int pk, int prec) { return pk == PK_VOIGT && prec == GEXS_FP32; }
+bool slices_apply(int, int) { return true; }
 
 long long slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows)
 {

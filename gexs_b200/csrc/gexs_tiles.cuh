@@ -769,20 +769,32 @@ tile_kernel(const KArgs args)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double zthr = (PREC == GEXS_FP32) ? 10.5 : 27.5;
 
+    const bool sliced = args.sl.prefix != nullptr;
+    const int nitems = sliced ? *(volatile const int*)args.sl.nitems : args.nitems;
+    __shared__ int s_last;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(args.counter, 1);
         __syncthreads();
         const int item = s_item;
-        if (item >= args.nitems) break;
+        if (item >= nitems) break;
+        /* item -> (tile, slice): one item per tile unless sliced */
+        int ti = item, sidx = 0, ns = 1;
+        if (sliced) {
+            int tl = 0, th = args.nitems;
+            while (th - tl > 1) { int m = (tl + th) >> 1; if (__ldg(args.sl.prefix + m) <= item) tl = m; else th = m; }
+            ti = tl;
+            sidx = item - __ldg(args.sl.prefix + tl);
+            ns = __ldg(args.sl.prefix + tl + 1) - __ldg(args.sl.prefix + tl);
+        }
 
-        /* job of this item: last prefix entry <= item */
+        /* job of this tile: last prefix entry <= tile */
         int jl = 0, jh = args.njobs;
-        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= item) jl = m; else jh = m; }
+        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
         Tile T;
         T.J = Jp;
-        T.j0 = J.start_idx + (int64_t)(item - __ldg(args.prefix + jl)) * W;
+        T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * W;
         T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
         T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
         T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
@@ -790,7 +802,15 @@ tile_kernel(const KArgs args)
 
         const int64_t nl = J.lines.count;
         const double margin = 2.0 * J.dnu + 1e-9 * (fabs(T.fl) + J.cutoff);
-        if (warp == 0) {
+        if (sliced) {
+            if (tid == 0) {
+                const long long tlo = __ldg(args.sl.lohi + 2 * ti), thi = __ldg(args.sl.lohi + 2 * ti + 1);
+                const long long per = (thi - tlo + ns - 1) / ns;
+                const long long a0 = tlo + (long long)sidx * per;
+                s_lohi[0] = min(a0, thi);
+                s_lohi[1] = min(a0 + per, thi);
+            }
+        } else if (warp == 0) {
             int64_t v = warp_bound<false>(J.lines.nu, nl, T.f0 - J.cutoff - margin, lane);
             if (lane == 0) s_lohi[0] = v;
         } else if (warp == 1) {
@@ -906,14 +926,45 @@ tile_kernel(const KArgs args)
         /* ------------------------------------------------------- write out */
         double* out = J.out;
         const int acc_mode = J.accumulate;
+        if (ns == 1) {
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
-            const int t = warp * 32 * B + lane + 32 * k;
-            if (t < T.jn) {
-                const double v = (PREC == GEXS_FP32) ? ((double)s_ks[t] - (double)s_kc[t]) : acc[k];
-                int64_t j = T.j0 + t;
-                out[j] = acc_mode ? out[j] + v : v;
+            for (int k = 0; k < B; ++k) {
+                const int t = warp * 32 * B + lane + 32 * k;
+                if (t < T.jn) {
+                    const double v = (PREC == GEXS_FP32) ? ((double)s_ks[t] - (double)s_kc[t]) : acc[k];
+                    int64_t j = T.j0 + t;
+                    out[j] = acc_mode ? out[j] + v : v;
+                }
             }
+        } else {
+            /* one slice of a split tile: its partial row, then a ticket; the
+             * last slice to finish adds the rows in slice order */
+            const int base = args.sl.prefix[ti];
+            const int rb = args.sl.rowbase[ti];
+            double* row = args.sl.rows + (size_t)(rb + sidx) * W;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = warp * 32 * B + lane + 32 * k;
+                if (t < T.jn) row[t] = (PREC == GEXS_FP32) ? ((double)s_ks[t] - (double)s_kc[t]) : acc[k];
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = atomicAdd(args.sl.ticket + ti, 1) == ns - 1;
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    if (t < T.jn) {
+                        double v = 0.0;
+                        for (int q = 0; q < ns; ++q) v += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
+                        int64_t j = T.j0 + t;
+                        out[j] = acc_mode ? out[j] + v : v;
+                    }
+                }
+            }
+            (void)base;
         }
         __syncthreads();
     }
@@ -1442,7 +1493,8 @@ static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStre
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     int per = ctas_per_sm > 0 ? min(ctas_per_sm, occ) : occ;
-    int grid = min(a.nitems, per * nsm);
+    /* sliced: the item count is known on the device only */
+    int grid = a.sl.prefix ? per * nsm : min(a.nitems, per * nsm);
     if (grid < 1) grid = 1;
     kern<<<grid, WARPS * 32, smem, st>>>(a);
     return cudaGetLastError();
@@ -1492,11 +1544,11 @@ static cudaError_t launch_ws(const KArgs& a, const gexs_launch_cfg& c, int nsm, 
 template <int PK, int PREC, bool PREP>
 static cudaError_t launch_cfg(const KArgs& a, const gexs_launch_cfg& c, int nsm, cudaStream_t st)
 {
+    if (a.sl.prefix) {
+        cudaError_t e = launch_slice_plan(a, st);
+        if (e != cudaSuccess) return e;
+    }
     if constexpr (PK == PK_VOIGT && PREC == GEXS_FP32) {
-        if (a.sl.prefix) {
-            cudaError_t e = launch_slice_plan(a, st);
-            if (e != cudaSuccess) return e;
-        }
         return launch_ws<PREP>(a, c, nsm, st);
     } else {
         if (c.bins_per_lane == 16) {
