@@ -12,9 +12,10 @@ int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
 /* Line slices of the tile kernels (the FP32 Voigt region-I kernel and
  * tile_kernel; not the FP32 Voigt core kernel): a tile whose line range
- * holds more than `lines_per_slice` lines is cut into ceil(n / lines_per_
- * slice) work items (the count depends on the tile alone, so the same tile
- * is cut the same way in every launch).  A split tile's slices write
+ * holds more than `lines_per_slice` lines (16384 unless the partial rows
+ * would pass 1 GiB) is cut into ceil(n / lines_per_slice) work items (the
+ * count depends on the tile alone, so the same tile is cut the same way
+ * in every launch).  A split tile's slices write
  * partial rows; the last one to finish sums them in slice order into the
  * output.  All arrays live in the launch table; slice_plan_kernel fills
  * them (and zeroes the tickets) before the region-I kernel runs. */
