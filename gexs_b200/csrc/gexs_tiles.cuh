@@ -6,7 +6,9 @@
  *
  * Work decomposition (replaces the reference's one-CTA-per-grid-point scan
  * over every line of a chunk, compute/CUDA/cross_kernal_v2.cu:403-457):
- *  - a work item is one tile of W = 32*B*WARPS consecutive bins of one job;
+ *  - a work item is one tile of W = 32*B*WARPS consecutive bins of one job,
+ *    or one slice of consecutive lines of a tile that holds more than the
+ *    launch's lines_per_slice (SliceTables, gexs_internal.h);
  *  - a persistent grid pulls items from a global counter;
  *  - the CTA finds the lines whose window can reach its tile with two
  *    warp-cooperative binary searches over the nu-sorted line list;
@@ -19,8 +21,9 @@
  *    reference CPU path, so FP32 evaluation never changes a window or a
  *    region decision;
  *  - lane l of warp w owns bins wb + l + 32k (k < B) in registers and loops
- *    over the stage's lines: no atomics, every bin sums its lines in
- *    ascending line order (deterministic, independent of other jobs);
+ *    over the stage's lines: no atomic accumulation, every bin sums its
+ *    lines in ascending line order, a split tile's slices are added in
+ *    slice order (deterministic, independent of other jobs);
  *  - FP32 form: FP32 partial sums of up to 128 lines merged into a
  *    Kahan-compensated (sum, compensation) pair per bin in shared memory;
  *    FP64 form: plain FP64 sums in registers.
