@@ -715,8 +715,9 @@ def our_arm(args):
             # per step: put_blob_kernel (launch table), prep_kernel (S(T),
             # width, y per line), slice_plan_kernel and slice_scan_kernel
             # (line slices), voigt_ws_kernel (region I), zero_ints_kernel
-            # (core work counter) and core_kernel (Humlicek regions II-IV)
-            "gpu_launches": 7 * args.steps,
+            # (core work counter), core_slice_plan_kernel and
+            # slice_scan_kernel (core slices), core_kernel (regions II-IV)
+            "gpu_launches": 9 * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": traffic,

@@ -165,6 +165,12 @@ struct Layout {
            os_rows = 0;
     int max_rows = 0;
     long long lines_per_slice = 0;
+    /* the FP32 Voigt core kernel's slice tables */
+    bool csliced = false;
+    size_t oc_prefix = 0, oc_counts = 0, oc_rowbase = 0, oc_ticket = 0, oc_lohi = 0, oc_nitems = 0,
+           oc_rows = 0;
+    int cmax_rows = 0;
+    long long clines_per_slice = 0;
 };
 
 static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg)
@@ -195,6 +201,17 @@ static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg
         L.os_lohi = up(a);   a = L.os_lohi + 2 * nt * sizeof(long long);
         L.os_nitems = up(a); a = L.os_nitems + 256;
         L.os_rows = up(a);   a = L.os_rows + (size_t)L.max_rows * W * sizeof(double);
+        if (core_slices_apply(g.pk, g.prec, W)) {
+            L.csliced = true;
+            L.clines_per_slice = core_slice_lines(g.jobs.data(), (int)g.jobs.size(), W, &L.cmax_rows);
+            L.oc_prefix = up(a); a = L.oc_prefix + (nt + 1) * sizeof(int);
+            L.oc_counts = up(a); a = L.oc_counts + nt * sizeof(int);
+            L.oc_rowbase = up(a); a = L.oc_rowbase + nt * sizeof(int);
+            L.oc_ticket = up(a); a = L.oc_ticket + nt * sizeof(int);
+            L.oc_lohi = up(a);   a = L.oc_lohi + 2 * nt * sizeof(long long);
+            L.oc_nitems = up(a); a = L.oc_nitems + 256;
+            L.oc_rows = up(a);   a = L.oc_rows + (size_t)L.cmax_rows * W * sizeof(double);
+        }
     }
     L.bytes = a + 256;
     return L;
@@ -240,9 +257,23 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
         sl.max_rows = L.max_rows;
         sl.lines_per_slice = L.lines_per_slice;
     }
+    SliceTables csl;
+    std::memset(&csl, 0, sizeof(csl));
+    if (L.csliced) {
+        csl.prefix = (int*)(d + L.oc_prefix);
+        csl.counts = (int*)(d + L.oc_counts);
+        csl.rowbase = (int*)(d + L.oc_rowbase);
+        csl.ticket = (int*)(d + L.oc_ticket);
+        csl.lohi = (long long*)(d + L.oc_lohi);
+        csl.nitems = (int*)(d + L.oc_nitems);
+        csl.rows = (double*)(d + L.oc_rows);
+        csl.max_rows = L.cmax_rows;
+        csl.lines_per_slice = L.clines_per_slice;
+    }
     return launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + L.op),
                         (int)g.jobs.size(), g.nitems, (int*)(d + L.oc), d_err,
-                        prep ? pp : nullptr, cfg, nsm, s, L.sliced ? &sl : nullptr);
+                        prep ? pp : nullptr, cfg, nsm, s, L.sliced ? &sl : nullptr,
+                        L.csliced ? &csl : nullptr);
 }
 
 extern "C" {

@@ -39,12 +39,19 @@ struct SliceTables {
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st, const SliceTables* sl = nullptr);
+                         cudaStream_t st, const SliceTables* sl = nullptr,
+                         const SliceTables* csl = nullptr);
 /* which groups are sliced (all); lines_per_slice for a group (grows only
  * when the partial rows of its split tiles could pass 1 GiB) and the bound
  * on those rows */
 bool slices_apply(int pk, int prec);
 long long slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows);
+/* the FP32 Voigt core kernel's own slices (its line range per tile is the
+ * lines whose core can reach the tile): only when a tile is one core
+ * sub-tile (tile_w <= 1024); 8192 lines per slice unless the rows, bounded
+ * by the core reach 15 nu dop_coef instead of the cutoff, would pass 1 GiB */
+bool core_slices_apply(int pk, int prec, int tile_w);
+long long core_slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows);
 cudaError_t launch_prep(const gexs_job* d_jobs, double* const* d_prep, int njobs,
                         int64_t max_lines, int nsm, cudaStream_t st);
 cudaError_t launch_count(const gexs_job* d_jobs, int njobs, unsigned long long* d_counts,

@@ -114,14 +114,16 @@ int profile_class(const gexs_job& j)
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st, const SliceTables* sl)
+                         cudaStream_t st, const SliceTables* sl, const SliceTables* csl)
 {
     KArgs a;
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
     a.counter = d_counter; a.err = d_err; a.prep = d_prep;
     a.tile_w = tile_bins(cfg);
     std::memset(&a.sl, 0, sizeof(a.sl));
+    std::memset(&a.csl, 0, sizeof(a.csl));
     if (sl && slices_apply(pk, prec)) a.sl = *sl;
+    if (csl && core_slices_apply(pk, prec, a.tile_w)) a.csl = *csl;
     switch (pk) {
     case PK_VOIGT: return launch_tiles_voigt(prec, a, cfg, nsm, st);
     case PK_ERF:   return launch_tiles_erf(prec, a, cfg, nsm, st);
@@ -169,6 +171,41 @@ __global__ void slice_plan_kernel(const KArgs a)
         a.sl.lohi[2 * ti + 1] = hi;
         a.sl.counts[ti] = n > per ? (int)((n + per - 1) / per) : 1;
         a.sl.ticket[ti] = 0;
+    }
+}
+
+/* the same for the FP32 Voigt core kernel: its line range per tile is the
+ * core kernel's own search (lines whose core, |f - nu| < 15 nu dop_coef,
+ * can reach the tile), computed with the same expressions */
+__global__ void core_slice_plan_kernel(const KArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ti >= a.nitems) return;
+    int jl = 0, jh = a.njobs;
+    while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
+    const gexs_job& J = a.jobs[jl];
+    const int64_t t0 = J.start_idx + (int64_t)(ti - __ldg(a.prefix + jl)) * a.tile_w;
+    const int64_t tend = min((int64_t)(t0 + a.tile_w), J.start_idx + J.n_points);
+    const int jn = (int)min((int64_t)CORE_W, tend - t0);
+    const double f0 = grid_f(J.nu_start, J.dnu, t0);
+    const double fl = grid_f(J.nu_start, J.dnu, t0 + jn - 1);
+    const int64_t nl = J.lines.count;
+    const double margin = 2.0 * J.dnu + 1e-9 * (fabs(fl) + J.cutoff);
+    const double k15 = 15.0 * J.dop_coef;
+    double vlo = f0 - J.cutoff, vhi = fl + J.cutoff;
+    vlo = fmax(vlo, f0 / (1.0 + k15));
+    if (k15 < 1.0) vhi = fmin(vhi, fl / (1.0 - k15));
+    vlo -= margin; vhi += margin;
+    if (vlo < 1e-6 + margin) vlo = -1.0;
+    const int64_t lo = warp_bound<false>(J.lines.nu, nl, vlo, lane);
+    const int64_t hi = max(warp_bound<true>(J.lines.nu, nl, vhi, lane), lo);
+    if (lane == 0) {
+        const long long n = hi - lo, per = a.csl.lines_per_slice;
+        a.csl.lohi[2 * ti] = lo;
+        a.csl.lohi[2 * ti + 1] = hi;
+        a.csl.counts[ti] = n > per ? (int)((n + per - 1) / per) : 1;
+        a.csl.ticket[ti] = 0;
     }
 }
 
@@ -221,7 +258,50 @@ cudaError_t launch_slice_plan(const KArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
+cudaError_t launch_core_slice_plan(const KArgs& a, cudaStream_t st)
+{
+    if (a.nitems <= 0) return cudaSuccess;
+    core_slice_plan_kernel<<<(a.nitems + 7) / 8, 256, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    KArgs c = a;
+    c.sl = a.csl;
+    slice_scan_kernel<<<1, 1024, 0, st>>>(c);
+    return cudaGetLastError();
+}
+
 bool slices_apply(int, int) { return true; }
+
+bool core_slices_apply(int pk, int prec, int tile_w)
+{
+    return pk == PK_VOIGT && prec == GEXS_FP32 && tile_w <= CORE_W;
+}
+
+long long core_slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows)
+{
+    /* as slice_lines, with a line's reach the core's: at most 15 nu
+     * dop_coef / (1 - 15 dop_coef) at the job's highest frequency, and at
+     * most the cutoff */
+    long long per = 8192;
+    for (;;) {
+        double rows = 0.0;
+        for (int i = 0; i < njobs; ++i) {
+            const gexs_job& j = jobs[i];
+            const double k15 = 15.0 * j.dop_coef;
+            const double nu_hi = j.nu_start + (double)(j.start_idx + j.n_points) * j.dnu + j.cutoff;
+            double reach = j.cutoff;
+            if (k15 < 1.0) reach = std::min(reach, nu_hi * k15 / (1.0 - k15));
+            const double tpl = std::floor((2.0 * reach + 8.0 * j.dnu) / ((double)tile_w * j.dnu)) + 3.0;
+            rows += 2.0 * std::ceil((double)j.lines.count * tpl / (double)per);
+        }
+        if (rows * tile_w * sizeof(double) <= (double)(1ull << 30)) {
+            *max_rows = (int)rows;
+            return per;
+        }
+        if (per >= (1ll << 40)) { *max_rows = 0; return 1ll << 62; }
+        per *= 2;
+    }
+}
 
 long long slice_lines(const gexs_job* jobs, int njobs, int tile_w, int* max_rows)
 {

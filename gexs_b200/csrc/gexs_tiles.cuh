@@ -314,11 +314,13 @@ struct KArgs {
     double* const*  prep;      /* per job S|invw|y arrays, or NULL       */
     int             tile_w;    /* bins per work item (core kernel)       */
     SliceTables     sl;        /* line slices (sl.prefix NULL: none)     */
+    SliceTables     csl;       /* FP32 Voigt core kernel's slices        */
 };
 
 /* slice_plan_kernel + slice_scan_kernel (gexs_kernels.cu): every tile's
  * line range and slice count, then the item prefix and count */
 cudaError_t launch_slice_plan(const KArgs& a, cudaStream_t st);
+cudaError_t launch_core_slice_plan(const KArgs& a, cudaStream_t st);
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
 {
@@ -1369,17 +1371,29 @@ core_kernel(const KArgs args)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* row = s_rows + warp * CORE_W;
+    /* sliced (host-enabled only when a tile is one sub-tile of CORE_W) */
+    const bool sliced = args.csl.prefix != nullptr;
+    const int nitems = sliced ? *(volatile const int*)args.csl.nitems : args.nitems;
+    __shared__ int s_last;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(args.counter, 1);
         __syncthreads();
         const int item = s_item;
-        if (item >= args.nitems) break;
+        if (item >= nitems) break;
+        int ti = item, sidx = 0, ns = 1;
+        if (sliced) {
+            int tl = 0, th = args.nitems;
+            while (th - tl > 1) { int m = (tl + th) >> 1; if (__ldg(args.csl.prefix + m) <= item) tl = m; else th = m; }
+            ti = tl;
+            sidx = item - __ldg(args.csl.prefix + tl);
+            ns = __ldg(args.csl.prefix + tl + 1) - __ldg(args.csl.prefix + tl);
+        }
         int jl = 0, jh = args.njobs;
-        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= item) jl = m; else jh = m; }
+        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
         /* the region-I kernel's tile of this item */
-        const int64_t t0 = J.start_idx + (int64_t)(item - __ldg(args.prefix + jl)) * args.tile_w;
+        const int64_t t0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * args.tile_w;
         const int64_t tend = min((int64_t)(t0 + args.tile_w), J.start_idx + J.n_points);
         const int64_t nl = J.lines.count;
         const double* pb = PREP ? args.prep[jl] : nullptr;
@@ -1399,7 +1413,16 @@ core_kernel(const KArgs args)
             if (k15 < 1.0) vhi = fmin(vhi, T.fl / (1.0 - k15));
             vlo -= margin; vhi += margin;
             if (vlo < 1e-6 + margin) vlo = -1.0;   /* nu == 0 lines count as 1e-6 */
-            if (warp == 0) {
+            if (sliced) {
+                /* the range from core_slice_plan_kernel, cut into ns parts */
+                if (tid == 0) {
+                    const long long tlo = __ldg(args.csl.lohi + 2 * ti), thi = __ldg(args.csl.lohi + 2 * ti + 1);
+                    const long long per = (thi - tlo + ns - 1) / ns;
+                    const long long a0 = tlo + (long long)sidx * per;
+                    s_lohi[0] = min(a0, thi);
+                    s_lohi[1] = min(a0 + per, thi);
+                }
+            } else if (warp == 0) {
                 int64_t v = warp_bound<false>(J.lines.nu, nl, vlo, lane);
                 if (lane == 0) s_lohi[0] = v;
             } else if (warp == 1) {
@@ -1466,17 +1489,44 @@ core_kernel(const KArgs args)
                 }
             }
             __syncthreads();
-            /* rows in warp order, added to the region-I result */
-            for (int t = tid; t < T.jn; t += NT) {
-                double v = 0.0;
-                bool any = false;
+            if (ns == 1) {
+                /* rows in warp order, added to the region-I result */
+                for (int t = tid; t < T.jn; t += NT) {
+                    double v = 0.0;
+                    bool any = false;
 #pragma unroll
-                for (int w = 0; w < CORE_WARPS; ++w) {
-                    const double r = s_rows[w * CORE_W + t];
-                    any |= (r != 0.0);
-                    v += r;
+                    for (int w = 0; w < CORE_WARPS; ++w) {
+                        const double r = s_rows[w * CORE_W + t];
+                        any |= (r != 0.0);
+                        v += r;
+                    }
+                    if (any) J.out[T.j0 + t] += v;
                 }
-                if (any) J.out[T.j0 + t] += v;
+            } else {
+                /* a slice of a split tile: rows in warp order into its partial
+                 * row, a ticket, and the last slice adds the partial rows in
+                 * slice order (a zero total adds nothing, as above) */
+                const int rb = args.csl.rowbase[ti];
+                const int W = args.tile_w;
+                double* prow = args.csl.rows + (size_t)(rb + sidx) * W;
+                for (int t = tid; t < T.jn; t += NT) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int w = 0; w < CORE_WARPS; ++w) v += s_rows[w * CORE_W + t];
+                    prow[t] = v;
+                }
+                __threadfence();
+                __syncthreads();
+                if (tid == 0) s_last = atomicAdd(args.csl.ticket + ti, 1) == ns - 1;
+                __syncthreads();
+                if (s_last) {
+                    __threadfence();
+                    for (int t = tid; t < T.jn; t += NT) {
+                        double v = 0.0;
+                        for (int q = 0; q < ns; ++q) v += __ldcg(args.csl.rows + (size_t)(rb + q) * W + t);
+                        if (v != 0.0) J.out[T.j0 + t] += v;
+                    }
+                }
             }
             __syncthreads();
         }
@@ -1590,11 +1640,16 @@ static cudaError_t launch_core(const KArgs& a, int nsm, cudaStream_t st)
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CORE_WARPS * 32, smem);
     if (e != cudaSuccess) return e;
-    const int grid = max(1, min(a.nitems, max(occ, 1) * nsm));
+    /* sliced: the item count is known on the device only */
+    const int grid = a.csl.prefix ? max(occ, 1) * nsm : max(1, min(a.nitems, max(occ, 1) * nsm));
     KArgs c = a;
     c.counter = a.counter + CORE_COUNTER_OFFSET;
     e = zero_ints(c.counter, 1, st);
     if (e != cudaSuccess) return e;
+    if (c.csl.prefix) {
+        e = launch_core_slice_plan(c, st);
+        if (e != cudaSuccess) return e;
+    }
     kern<<<grid, CORE_WARPS * 32, smem, st>>>(c);
     return cudaGetLastError();
 }
