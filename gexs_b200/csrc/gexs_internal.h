@@ -11,7 +11,8 @@ namespace gexs {
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
 /* Line slices of the tile kernels (the FP32 Voigt region-I kernel and
- * tile_kernel; not the FP32 Voigt core kernel): a tile whose line range
+ * tile_kernel; the FP32 Voigt core kernel has its own, below): a tile
+ * whose line range
  * holds more than `lines_per_slice` lines (16384 unless the partial rows
  * would pass 1 GiB) is cut into ceil(n / lines_per_slice) work items (the
  * count depends on the tile alone, so the same tile is cut the same way
