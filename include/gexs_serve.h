@@ -58,7 +58,11 @@ typedef struct gexs_request_info {
 /* device: CUDA device; hbm_budget: bytes the server may use for resident
  * lists plus in-flight outputs (0 = 90% of free memory); max_inflight:
  * admitted-but-unfetched requests at most (0 = 256); streams: launch
- * streams (0 = 4). */
+ * streams (0 = 4).  Each launch's scratch is not part of the budget: it
+ * comes from the context's memory pool, 24 B per line of prep arrays plus
+ * the line-slice tables (at most 1 GiB of partial rows for region I and
+ * 1 GiB for the Voigt core), so leave that much outside the budget per
+ * stream. */
 int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int streams,
                        gexs_server** out);
 int gexs_server_destroy(gexs_server* s);
