@@ -50,7 +50,9 @@ public:
      * GEXS_CONV_REF_CPU OpenMPManager's, GEXS_CONV_PHYSICAL the corrected
      * one.  precision: GEXS_FP64 or GEXS_FP32.  memory_bytes bounds the
      * device memory taken for lines and result slots (0: half the free
-     * memory), which sets GetNtrans(). */
+     * memory), which sets GetNtrans().  Each launch's scratch (24 B per
+     * line of prep arrays, the line-slice tables) comes on top of it from
+     * the context's memory pool. */
     B200Manager(ProfileType profile, int device = 0, int convention = GEXS_CONV_REF_GPU,
                 int precision = GEXS_FP64, size_t memory_bytes = 0);
     ~B200Manager();
