@@ -164,51 +164,105 @@ def gpu_reference_sample(torch, ctx, L, q, dev, k=1_000_000, reps=3):
                                "__shfl_xor_sync (oracle/ref_gpu_shim.h), nothing else changed"}
 
 
-def cpu_reference_sample(target_s=12.0, seed_states=1002, seed_lines=2002):
-    """Reference CPU path (OpenMPManager::ComputeVoigtTP + humlic, compiled
-    from the reference sources at -O3 -march=x86-64-v3) on a bounded sample
-    of the Voigt workload's distribution, all host threads.  Returns
-    (evals/s, threads, sample description, kind)."""
-    from gexs_b200 import synth
-    from oracle import pyoracle as po
-    from gexs_b200 import _capi as capi
-    from gexs_b200.engine import job_init
-    from tests.helpers import host_job
-    kind = "reference" if po.ref_available(fast=True) else "port"
-    threads = len(os.sched_getaffinity(0))
-    st = synth.make_states(200000, 80, seed_states)
-    L = synth.make_lines(st, 2000000, NU0, NU1, seed_lines, broadening_seed=seed_lines + 1000)
-    q = po.partition(st.energy, st.g, T_K)
+def _synth():
+    """The numpy workload generator (gexs_b200/synth.py) loaded by file path,
+    so the reference arm imports nothing of the gexs_b200 package (whose
+    import would map libgexs_b200.so)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "gexs_workload_synth", os.path.join(ROOT, "gexs_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
-    def run(k):
-        mid = len(L["nu"]) // 2
+
+def reference_window_evals(nu, f0, dnu, nb, cut):
+    """(line, bin) pairs the reference CPU loop visits: bins [ib, ie) with
+    ib = max(round((nu-cut-f0)/dnu), 0), ie = min(round((nu+cut-f0)/dnu), nb)
+    (Managers/CPU/OpenMPManager.cpp:399-400; C round, half away from zero),
+    for every line (all synthetic A > 0, so no line is skipped at :402)."""
+    nu = np.where(nu == 0.0, 1e-6, nu)
+
+    def cround(x):
+        return np.copysign(np.floor(np.abs(x) + 0.5), x)
+    ib = np.maximum(cround((nu - cut - f0) / dnu), 0.0)
+    ie = np.minimum(cround((nu + cut - f0) / dnu), float(nb))
+    return int(np.sum(np.maximum(ie - ib, 0.0)))
+
+
+class ReferenceSample:
+    """The reference CPU path (OpenMPManager::ComputeVoigtTP + humlic,
+    compiled from the reference sources at -O3 -march=x86-64-v3 into
+    oracle/_ref/libgexsref_fast.so; the FP64 port in oracle/ when that
+    build is absent) on a bounded sample of the Voigt workload: k
+    consecutive lines around the median nu0 of a 2e6-line list with the
+    workload's distribution (2e5 states, J 0-80, nu0 100-30000) over the
+    bins of their window, all host threads.  The list is generated once; k
+    is sized once so that one pass takes about target_s seconds."""
+
+    def __init__(self, target_s, seed_states=1002, seed_lines=2002):
+        from oracle import pyoracle as po
+        self.po = po
+        if not os.path.exists(po.ORACLE_LIB) and not po.ref_available(fast=True):
+            po.build(with_reference=False)
+        self.kind = "reference" if po.ref_available(fast=True) else "port"
+        self.threads = len(os.sched_getaffinity(0))
+        sy = _synth()
+        st = sy.make_states(200000, 80, seed_states)
+        self.L = sy.make_lines(st, 2000000, NU0, NU1, seed_lines, broadening_seed=seed_lines + 1000)
+        self.q = (po.ref_partition(st.energy, st.g, T_K, fast=True) if self.kind == "reference"
+                  else po.partition(st.energy, st.g, T_K))
+        k = 2000
+        dt = self._prepare(k)
+        while dt < 0.5 and k < len(self.L["nu"]) // 2:
+            k *= 4
+            dt = self._prepare(k)
+        k = int(min(len(self.L["nu"]) - 2, k * max(1.0, target_s / max(dt, 1e-3))))
+        self._prepare(k, timed=False)
+
+    def _prepare(self, k, timed=True):
+        mid = len(self.L["nu"]) // 2
         sl = slice(mid - k // 2, mid - k // 2 + k)
-        S = {kk: np.ascontiguousarray(v[sl]) for kk, v in L.items()}
-        lo = S["nu"][0] - CUT - 1.0
-        nb = int((S["nu"][-1] + CUT + 1.0 - lo) / DNU) + 1
-        freq = lo + np.arange(nb, dtype=np.float64) * DNU
-        j = job_init(capi.CONV_REF_CPU, capi.VOIGT, T_K, P_BAR, q, MASS, lo, DNU, nb,
-                     ref_temp=296.0)
-        ev = po.count_evals(host_job(j, S))
-        t0 = time.perf_counter()
-        if kind == "reference":
-            po.ref_voigt_tp(freq, S, T_K, P_BAR, q, MASS, 296.0, DNU, nthreads=threads, fast=True)
-        else:
-            po.cross_section(host_job(j, S), nthreads=threads)
-        return ev, time.perf_counter() - t0
+        self.S = {kk: np.ascontiguousarray(v[sl]) for kk, v in self.L.items()}
+        self.lo = float(self.S["nu"][0]) - CUT - 1.0
+        self.nb = int((float(self.S["nu"][-1]) + CUT + 1.0 - self.lo) / DNU) + 1
+        self.freq = self.lo + np.arange(self.nb, dtype=np.float64) * DNU
+        self.k = k
+        # reference CPU convention at P = 1 bar: cutoff min(25 P, 100) = 25
+        self.evals = reference_window_evals(self.S["nu"], self.lo, DNU, self.nb,
+                                            min(25.0 * P_BAR, 100.0))
+        return self.run() if timed else 0.0
 
-    k = 2000
-    ev, dt = run(k)
-    while dt < 0.5 and k < len(L["nu"]) // 2:
-        k *= 4
-        ev, dt = run(k)
-    rate = ev / dt
-    k = int(min(len(L["nu"]) - 2, k * max(1.0, target_s / max(dt, 1e-3))))
-    ev, dt = run(k)
-    sample = ("%d consecutive lines around the median nu0 of a 2e6-line list with the "
-              "workload's distribution; %.3g evaluations in %.1f s (reference CPU "
-              "conventions: HWHM Doppler scaling, cutoff min(25P,100)=25)" % (k, ev, dt))
-    return ev / dt, threads, sample, kind
+    def run(self):
+        """one pass; returns its wall time in s"""
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            self.po.ref_voigt_tp(self.freq, self.S, T_K, P_BAR, self.q, MASS, 296.0, DNU,
+                                 nthreads=self.threads, fast=True)
+        else:
+            self.po.cross_section(self._port_job(), nthreads=self.threads)
+        return time.perf_counter() - t0
+
+    def _port_job(self):
+        from gexs_b200 import _capi as capi
+        from gexs_b200.engine import job_init
+        from tests.helpers import host_job
+        j = job_init(capi.CONV_REF_CPU, capi.VOIGT, T_K, P_BAR, self.q, MASS, self.lo, DNU,
+                     self.nb, ref_temp=296.0)
+        return host_job(j, self.S)
+
+    def describe(self, dt):
+        return ("%d consecutive lines around the median nu0 of a 2e6-line list with the "
+                "workload's distribution, %d bins; %.4g evaluations per pass, %.2f s per pass "
+                "(reference CPU conventions: HWHM Doppler scaling, cutoff min(25P,100)=25)"
+                % (self.k, self.nb, self.evals, dt))
+
+
+def cpu_reference_sample(target_s=12.0):
+    """(evals/s, threads, sample description, kind) of one pass."""
+    R = ReferenceSample(target_s)
+    dt = R.run()
+    return R.evals / dt, R.threads, R.describe(dt), R.kind
 
 
 def reference_arm(args):
@@ -217,31 +271,32 @@ def reference_arm(args):
         return 0
     try:
         from oracle import pyoracle as po
-        if not os.path.exists(po.ORACLE_LIB):
+        if not po.ref_available(fast=True) and not os.path.exists(po.ORACLE_LIB):
             po.build(with_reference=False)
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": "CPU checker build failed: %s" % e}))
         return 0
-    rates = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        r, threads, sample, kind = cpu_reference_sample(target_s=args.cpu_seconds)
-        info = (threads, sample, kind)
-        if i >= args.warmup:
-            rates.append(r)
-    value = float(np.mean(rates))
-    evals_per_step = value * args.cpu_seconds
+    # the whole run (warm-up + timed passes) stays within about three minutes
+    per = max(0.5, min(args.cpu_seconds, 180.0 / (args.steps + args.warmup)))
+    R = ReferenceSample(per)
+    for _ in range(args.warmup):
+        R.run()
+    times = [R.run() for _ in range(args.steps)]
+    total = float(np.sum(times))
+    value = R.evals * args.steps / total
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * args.cpu_seconds, "higher_is_better": True,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "Voigt, 1e8-line list distribution, T=1500 K, P=1 bar, "
-                                   "0.01 cm^-1 grid, cutoff 25 (bounded CPU sample per step)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[0], "kind": info[2],
-                             "sample": info[1]},
+                                   "0.01 cm^-1 grid, cutoff 25 (bounded CPU sample per step)",
+                       "evals_per_step": R.evals, "lines_per_step": R.k,
+                       "bins_per_step": R.nb},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": R.threads, "kind": R.kind,
+                             "sample": R.describe(total / args.steps)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "evals_per_step": evals_per_step}
+            "timed": "wall clock of each pass of the reference CPU loop on the sample"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -264,6 +319,39 @@ def region_flops(L, q):
     hist = np.array(po.region_hist(host_job(j, S)), dtype=np.float64)
     frac = hist / hist.sum()
     return float(np.dot(frac, FLOPS_REGION)), [float(f) for f in frac]
+
+
+def oracle_subband(torch, L, q, outs, nbins=2000):
+    """Error of the device results against the FP64 oracle (oracle/,
+    checker only) on `nbins` bins around the median nu0 of the list: the
+    oracle evaluates the same job restricted to those bins (start_idx,
+    n_points) over the lines that can reach them.  outs: {name: (device
+    grid, precision)}."""
+    from gexs_b200 import _capi as capi
+    from gexs_b200.engine import job_init
+    from oracle import pyoracle as po
+    from tests.helpers import host_job, fp32_errors
+    nu = L["nu"]
+    mid = float(nu[nu.shape[0] // 2])
+    j0 = int(round((mid - NU0) / DNU)) - nbins // 2
+    fa, fb = NU0 + j0 * DNU, NU0 + (j0 + nbins - 1) * DNU
+    a = int(torch.searchsorted(nu, torch.tensor(fa - CUT - 1.0, dtype=nu.dtype, device=nu.device)))
+    b = int(torch.searchsorted(nu, torch.tensor(fb + CUT + 1.0, dtype=nu.dtype, device=nu.device)))
+    S = {k: np.ascontiguousarray(v[a:b].cpu().numpy()) for k, v in L.items()}
+    j = job_init(capi.CONV_PHYSICAL, capi.VOIGT, T_K, P_BAR, q, MASS, NU0, DNU, grid_points(),
+                 cutoff=CUT)
+    j.start_idx, j.n_points = j0, nbins
+    ref = po.cross_section(host_job(j, S), nthreads=len(os.sched_getaffinity(0)))[j0:j0 + nbins]
+    res = {"bins": nbins, "lines": b - a, "nu_range": [fa, fb]}
+    for name, (o, prec) in outs.items():
+        got = o[j0:j0 + nbins].cpu().numpy()
+        if prec == capi.FP64:
+            res[name + "_max_rel_vs_oracle"] = float(np.max(np.abs(got - ref) / np.abs(ref)))
+        else:
+            rel, band = fp32_errors(got, ref)
+            res[name + "_max_rel_vs_oracle_bins_gt_1e-6_peak"] = rel
+            res[name + "_band_rel_vs_oracle"] = band
+    return res
 
 
 def batch64(ctx, torch, dev):
@@ -460,10 +548,11 @@ def quad_suite(args):
     del L
     torch.cuda.empty_cache()
     T = 2500.0
-    q = po.partition(st.energy, st.g, T)
+    ctx = Context(0)
+    q = float(ctx.partition(torch.as_tensor(st.energy, device=dev),
+                            torch.as_tensor(st.g, dtype=torch.int32, device=dev), [T])[0])
     nu0, d = 10.0, 0.01
     G = int(round((20000.0 - nu0) / d)) + 1
-    ctx = Context(0)
     out = torch.zeros(G, dtype=torch.float64, device=dev)
     ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sub0 = int(round((5000.0 - nu0) / d))
@@ -596,17 +685,16 @@ def our_arm(args):
     dev = "cuda:%d" % local_rank
     torch.cuda.set_device(local_rank)
     from gexs_b200 import Context, Job, LineList, synth, _capi as capi
-    from oracle import pyoracle as po
-    if not os.path.exists(po.ORACLE_LIB):
-        po.build(with_reference=False)
 
     st = synth.make_states(200000, 80, 1002)
     L = synth.make_lines_torch(st, args.lines, NU0, NU1, 2002, broadening_seed=3002, device=dev)
     lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev)
-    q = po.partition(st.energy, st.g, T_K)
     G = grid_points()
     out = torch.zeros(G, dtype=torch.float64, device=dev)
     ctx = Context(local_rank)
+    # Q(T) by the product's own device reduction (gexs_partition)
+    q = float(ctx.partition(torch.as_tensor(st.energy, device=dev),
+                            torch.as_tensor(st.g, dtype=torch.int32, device=dev), [T_K])[0])
     start_idx, n_points = 0, G
     if args.shard == "grid" and ws > 1:
         from gexs_b200 import shard
@@ -666,6 +754,10 @@ def our_arm(args):
     fp32_err = float(((out[msk] - out64[msk]).abs() / out64[msk]).max())
     band_err = abs(float(out.sum()) - float(out64.sum())) / float(out64.sum())
     integral = float(out64.sum()) * DNU
+    vs_oracle = None
+    if rank == 0 and not args.no_cpu and (start_idx, n_points) == (0, G):
+        vs_oracle = oracle_subband(torch, L, q, {"fp32": (out, capi.FP32),
+                                                 "fp64": (out64, capi.FP64)})
     del out64, j64
 
     # e2e through the manager C ABI, host buffers
@@ -737,7 +829,8 @@ def our_arm(args):
             "fp64_plain": {"ms": fp64_ms, "evals_per_s": evals / (fp64_ms * 1e-3),
                            "fp32_speedup": fp64_ms / launch_ms},
             "accuracy": {"fp32_max_rel_vs_fp64_bins_gt_1e-6_peak": fp32_err,
-                         "fp32_band_rel_vs_fp64": band_err, "integrated_fp64": integral},
+                         "fp32_band_rel_vs_fp64": band_err, "integrated_fp64": integral,
+                         "vs_oracle_subband": vs_oracle},
             "clocks": clocks,
         }
     if not args.no_cpu and rank == 0 and ws == 1:

@@ -14,6 +14,8 @@ GEXS_ERR_INVALID = -1
 GEXS_ERR_TIMEOUT = -4
 GEXS_ERR_NOT_READY = -5
 GEXS_ERR_ADMISSION = -6
+GEXS_ERR_KERNEL = -8
+KERR_PIPELINE = 1
 NOALLOC_MAX_JOBS = 64
 
 GAUSSIAN, DOPPLER, VOIGT, VOIGT_QUAD = 0, 1, 2, 4
@@ -44,7 +46,7 @@ class GexsJob(C.Structure):
 
 class GexsLaunchCfg(C.Structure):
     _fields_ = [("bins_per_lane", C.c_int32), ("warps", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("flags", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("flags", C.c_int32), ("wait_spins", C.c_int32)]
 
 LAUNCH_DERIVE_ON_LOAD = 1
 
@@ -93,6 +95,7 @@ SIGNATURES = [
     ("gexs_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
     ("gexs_run_noalloc", C.c_int, [C.POINTER(GexsJob), C.c_int, C.POINTER(GexsLaunchCfg),
                                    C.c_void_p]),
+    ("gexs_noalloc_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("gexs_run", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,
                            C.POINTER(GexsLaunchCfg), C.c_void_p]),
     ("gexs_count_evals", C.c_int, [C.c_void_p, C.POINTER(GexsJob), C.c_int,

@@ -70,7 +70,7 @@ using namespace gexs;
 struct gexs_ctx {
     int device = 0;
     int nsm = 148;
-    int* d_err = nullptr;            /* sticky kernel error word */
+    int* d_err = nullptr;            /* kernel error word; d_err[1]: its last reading */
     /* launch tables and per-line prep arrays: kept mapped between calls (no
      * release threshold) and never made to wait on a free from another
      * stream (no internal dependencies), so calls on two streams overlap */
@@ -89,7 +89,7 @@ static gexs_launch_cfg default_cfg(int pk, int prec)
     /* measured best on B200 for the 1e8-line Voigt workload (FP32: 4 bins x
      * 4 warps, FP64: 4 x 8); gexs_autotune replaces it per (profile,
      * precision) */
-    gexs_launch_cfg c;
+    gexs_launch_cfg c{};
     c.bins_per_lane = 4;
     c.warps = (prec == GEXS_FP64) ? 8 : 4;
     c.ctas_per_sm = 0;
@@ -103,7 +103,7 @@ static bool cfg_ok(const gexs_launch_cfg& c, int prec)
     /* 16 bins per lane only for the FP32 form */
     return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8 ||
             (c.bins_per_lane == 16 && prec == GEXS_FP32)) &&
-           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0;
+           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0;
 }
 
 static gexs_launch_cfg ctx_cfg(gexs_ctx* ctx, int pk, int prec)
@@ -383,9 +383,9 @@ int gexs_ctx_create(int device, gexs_ctx** out)
     c->device = device;
     e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) { delete c; return cuda_error(e, "cudaDeviceGetAttribute"); }
-    e = cudaMalloc(&c->d_err, sizeof(int));
+    e = cudaMalloc(&c->d_err, 2 * sizeof(int));
     if (e != cudaSuccess) { delete c; return set_error(GEXS_ERR_OOM, "error word"); }
-    cudaMemset(c->d_err, 0, sizeof(int));
+    cudaMemset(c->d_err, 0, 2 * sizeof(int));
     cudaMemPoolProps props;
     std::memset(&props, 0, sizeof(props));
     props.allocType = cudaMemAllocationTypePinned;
@@ -420,10 +420,16 @@ int gexs_ctx_destroy(gexs_ctx* ctx)
 int gexs_ctx_check(gexs_ctx* ctx, void* stream)
 {
     if (!ctx) return set_error(GEXS_ERR_INVALID, "ctx is NULL");
-    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
     int flag = 0;
-    e = cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    /* one reading slot per context: checks from several threads take turns */
+    std::lock_guard<std::mutex> g(ctx->mu);
+    e = take_word(ctx->d_err, ctx->d_err + 1, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, ctx->d_err + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "read error word");
     if (flag) return set_error(GEXS_ERR_KERNEL, "kernel error flag " + std::to_string(flag));
     return GEXS_OK;
@@ -433,6 +439,16 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
              void* stream)
 {
     if (!ctx) return set_error(GEXS_ERR_INVALID, "ctx is NULL");
+    return gexs::run_jobs(ctx, jobs, njobs, cfg, stream, nullptr);
+}
+
+}  // extern "C"
+
+int gexs::run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
+                   void* stream, int* d_err)
+{
+    if (!ctx) return set_error(GEXS_ERR_INVALID, "ctx is NULL");
+    if (!d_err) d_err = ctx->d_err;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
     std::vector<Group> groups;
@@ -453,12 +469,14 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
         std::vector<unsigned char> h = group_image(g, L, (unsigned char*)d, prep);
         e = put_bytes(d, h.data(), h.size(), s);
         if (e != cudaSuccess) { cudaFreeAsync(d, s); return cuda_error(e, "upload launch tables"); }
-        e = enqueue_group(g, L, (unsigned char*)d, prep, cfgs[gi], ctx->d_err, ctx->nsm, s);
+        e = enqueue_group(g, L, (unsigned char*)d, prep, cfgs[gi], d_err, ctx->nsm, s);
         cudaFreeAsync(d, s);
         if (e != cudaSuccess) return cuda_error(e, "tile kernel launch");
     }
     return GEXS_OK;
 }
+
+extern "C" {
 
 int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs, int64_t* h_counts)
 {
@@ -610,7 +628,7 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
     int st = GEXS_OK;
     for (int bi = 0; bi < nbins && !st; ++bi)
         for (int wi = 0; wi < 2 && !st; ++wi) {
-            gexs_launch_cfg c; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
+            gexs_launch_cfg c{}; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
             c.ctas_per_sm = 0; c.flags = 0;
             gexs_batch* b = nullptr;
             st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);

@@ -68,6 +68,13 @@ cudaError_t launch_partition(const double* d_e, const int32_t* d_g, int64_t n,
 const size_t kMaxParamUpload = 64 * 1024;
 cudaError_t put_bytes(void* dst, const void* src, size_t n, cudaStream_t st);
 cudaError_t zero_ints(int* p, int n, cudaStream_t st);
+/* *out = the error word, which is set to zero in the same atomic step */
+cudaError_t take_word(int* word, int* out, cudaStream_t st);
+
+/* gexs_run with the kernels' error flags going to d_err (device int)
+ * instead of the context's own word (NULL: the context's) */
+int run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
+             void* stream, int* d_err);
 
 /* context accessors (gexs_capi.cu) */
 int ctx_device(gexs_ctx* c);

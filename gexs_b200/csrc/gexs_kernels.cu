@@ -120,6 +120,7 @@ cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
     a.counter = d_counter; a.err = d_err; a.prep = d_prep;
     a.tile_w = tile_bins(cfg);
+    a.spin = cfg.wait_spins > 0 ? cfg.wait_spins : WS_SPIN;
     std::memset(&a.sl, 0, sizeof(a.sl));
     std::memset(&a.csl, 0, sizeof(a.csl));
     if (sl && slices_apply(pk, prec)) a.sl = *sl;
@@ -344,7 +345,18 @@ __global__ void zero_ints_kernel(int* p, int n)
 {
     for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0;
 }
+
+__global__ void take_word_kernel(int* word, int* out)
+{
+    *out = atomicExch(word, 0);
+}
 }  // namespace
+
+cudaError_t take_word(int* word, int* out, cudaStream_t st)
+{
+    take_word_kernel<<<1, 1, 0, st>>>(word, out);
+    return cudaGetLastError();
+}
 
 cudaError_t put_bytes(void* dst, const void* src, size_t n, cudaStream_t st)
 {

@@ -26,9 +26,10 @@ constexpr int kMaxDevices = 64;
 constexpr size_t kJobsBytes = sizeof(gexs_job) * GEXS_NOALLOC_MAX_JOBS;
 constexpr size_t kPrefixOff = (kJobsBytes + 255) & ~size_t(255);
 constexpr size_t kCounterOff = (kPrefixOff + sizeof(int) * (GEXS_NOALLOC_MAX_JOBS + 1) + 255) & ~size_t(255);
-constexpr size_t kErrOff = kCounterOff + 256;
+constexpr size_t kErrOff = kCounterOff + 256;   /* kernel error word of the last call */
 constexpr size_t kScratchBytes = kErrOff + 256;
 static_assert(kScratchBytes <= GEXS_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds its array");
+static_assert(kJobsBytes <= gexs::kMaxParamUpload, "the job table must fit in kernel parameters");
 
 /* Host code must never pass this name to a kernel: on the host it is a
  * stand-in symbol, not a device address.  Its device address comes from
@@ -63,19 +64,22 @@ extern "C" int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_laun
     if (!jobs || njobs < 1 || njobs > GEXS_NOALLOC_MAX_JOBS)
         return set_error(GEXS_ERR_INVALID, "gexs_run_noalloc: njobs must be 1.." +
                                                std::to_string(GEXS_NOALLOC_MAX_JOBS));
-    gexs_launch_cfg c;
-    c.bins_per_lane = 4; c.warps = 8; c.ctas_per_sm = 0; c.flags = GEXS_LAUNCH_DERIVE_ON_LOAD;
+    const int pk = profile_class(jobs[0]), prec = jobs[0].precision;
+    /* gexs_run's defaults: 4 bins per lane, 4 warps (FP32) or 8 (FP64) */
+    gexs_launch_cfg c{};
+    c.bins_per_lane = 4; c.warps = (prec == GEXS_FP64) ? 8 : 4;
     if (cfg) c = *cfg;
+    /* no per-job prep arrays: every line is derived as it is loaded */
+    c.flags |= GEXS_LAUNCH_DERIVE_ON_LOAD;
     if (!((c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8) &&
-          (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0))
+          (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0))
         return set_error(GEXS_ERR_INVALID, "gexs_run_noalloc: launch configuration");
 
-    /* host image on the stack: job table and tile prefix sums */
+    /* host image: job table and tile prefix sums */
     struct Image {
         gexs_job jobs[GEXS_NOALLOC_MAX_JOBS];
         int prefix[GEXS_NOALLOC_MAX_JOBS + 1];
     } img;
-    const int pk = profile_class(jobs[0]), prec = jobs[0].precision;
     const int W = tile_bins(c);
     int64_t nitems = 0;
     img.prefix[0] = 0;
@@ -104,16 +108,39 @@ extern "C" int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_laun
     if (e != cudaSuccess) return cuda_error(e, "gexs_run_noalloc: cudaDeviceGetAttribute");
 
     cudaStream_t s = (cudaStream_t)stream;
-    e = cudaMemcpyAsync(base, img.jobs, sizeof(gexs_job) * njobs, cudaMemcpyHostToDevice, s);
+    /* the tables travel as kernel parameters (put_bytes), so the call
+     * reads nothing from host memory once it has returned */
+    e = put_bytes(base, img.jobs, sizeof(gexs_job) * njobs, s);
+    if (e == cudaSuccess) e = put_bytes(base + kPrefixOff, img.prefix, sizeof(int) * (njobs + 1), s);
+    /* the work counter and the error word start at zero on every call */
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(base + kPrefixOff, img.prefix, sizeof(int) * (njobs + 1),
-                            cudaMemcpyHostToDevice, s);
-    /* the work counter must start at zero on every call */
-    if (e == cudaSuccess) e = cudaMemsetAsync(base + kCounterOff, 0, sizeof(int), s);
+        e = zero_ints((int*)(base + kCounterOff), (int)((kErrOff - kCounterOff) / sizeof(int)) + 1, s);
     if (e != cudaSuccess) return cuda_error(e, "gexs_run_noalloc: upload launch tables");
     e = launch_tiles(pk, prec, (const gexs_job*)base, (const int*)(base + kPrefixOff), njobs,
                      (int)nitems, (int*)(base + kCounterOff), (int*)(base + kErrOff), nullptr, c, nsm,
                      s);
     if (e != cudaSuccess) return cuda_error(e, "gexs_run_noalloc: tile kernel launch");
+    return GEXS_OK;
+}
+
+extern "C" int gexs_noalloc_status(void* stream, int* flags)
+{
+    using namespace gexs;
+    if (!flags) return set_error(GEXS_ERR_INVALID, "gexs_noalloc_status: flags is NULL");
+    *flags = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "gexs_noalloc_status: cudaGetDevice");
+    unsigned char* base = nullptr;
+    int st = scratch_address(dev, &base);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    int word = 0;
+    e = cudaMemcpyAsync(&word, base + kErrOff, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "gexs_noalloc_status: read error word");
+    *flags = word;
+    if (word)
+        return set_error(GEXS_ERR_KERNEL, "gexs_run_noalloc: kernel error flags " + std::to_string(word));
     return GEXS_OK;
 }

@@ -315,6 +315,7 @@ struct KArgs {
     int             tile_w;    /* bins per work item (core kernel)       */
     SliceTables     sl;        /* line slices (sl.prefix NULL: none)     */
     SliceTables     csl;       /* FP32 Voigt core kernel's slices        */
+    int             spin;      /* try_wait attempts of every bounded wait */
 };
 
 /* slice_plan_kernel + slice_scan_kernel (gexs_kernels.cu): every tile's
@@ -992,9 +993,7 @@ tile_kernel(const KArgs args)
  * the bins out.  Each bin still sums its lines in ascending order. */
 constexpr int WS_STAGES = 4;
 constexpr int WS_R = 128;
-constexpr int WS_SPIN = 1 << 21;          /* try_wait attempts before giving up */
-constexpr int GEXS_KERR_PIPELINE = 1;
-constexpr int GEXS_KERR_SLICES = 2;     /* more line slices than the tables hold */
+constexpr int WS_SPIN = 1 << 21;          /* default try_wait attempts before giving up */
 
 struct StageHdr {
     long long j0;          /* absolute first bin of the tile                */
@@ -1021,11 +1020,11 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* b)
 /* bounded wait for the completion of the phase with parity `parity`; a
  * waiting warp backs off (nanosleep, doubling up to 256 ns) so that it does
  * not take issue slots from the warps that do the work */
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, int limit)
 {
     const unsigned a = smem_u32(b);
     unsigned ns = 16;
-    for (int it = 0; it < WS_SPIN; ++it) {
+    for (int it = 0; it < limit; ++it) {
         unsigned ok;
         asm volatile("{\n\t.reg .pred p;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -1099,7 +1098,7 @@ voigt_ws_kernel(const KArgs args)
         /* barrier among the producer threads, bounded like every wait here */
         auto psync = [&]() -> bool {
             mbar_arrive(s_pbar);
-            const bool ok = mbar_wait(s_pbar, pph);
+            const bool ok = mbar_wait(s_pbar, pph, args.spin);
             pph ^= 1;
             return ok;
         };
@@ -1108,7 +1107,7 @@ voigt_ws_kernel(const KArgs args)
             if (!psync()) { fail(); return; }
             const int item = s_item;
             if (item >= nitems) {
-                if (!mbar_wait(s_empty + st, ph)) { fail(); return; }
+                if (!mbar_wait(s_empty + st, ph, args.spin)) { fail(); return; }
                 if (ptid == 0) { s_hdr[st].flags = 4; s_hdr[st].nrec = 0; }
                 mbar_arrive(s_full + st);
                 return;
@@ -1185,7 +1184,7 @@ voigt_ws_kernel(const KArgs args)
             issue(0);
             issue(1);
             for (int c = 0; c < nchunk; ++c) {
-                if (!mbar_wait(s_empty + st, ph)) { fail(); return; }
+                if (!mbar_wait(s_empty + st, ph, args.spin)) { fail(); return; }
                 const int64_t pbase = lo + (int64_t)c * WS_R;
                 const int nrec = (int)max((int64_t)0, min((int64_t)WS_R, hi - pbase));
                 RecV* rec = s_rec + st * WS_R;
@@ -1240,7 +1239,7 @@ voigt_ws_kernel(const KArgs args)
     auto csync = [&]() -> bool {
         __syncwarp();
         if (lane == 0) mbar_arrive(s_pbar + 1);
-        const bool ok = mbar_wait(s_pbar + 1, cph);
+        const bool ok = mbar_wait(s_pbar + 1, cph, args.spin);
         cph ^= 1;
         return ok;
     };
@@ -1248,7 +1247,7 @@ voigt_ws_kernel(const KArgs args)
 #pragma unroll
     for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
     for (;;) {
-        if (!mbar_wait(s_full + st, ph)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+        if (!mbar_wait(s_full + st, ph, args.spin)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
         const StageHdr h = s_hdr[st];
         if (h.flags & 4) return;
         if (h.flags & 1) {

@@ -110,7 +110,8 @@ def _cfg(cfg):
     if isinstance(cfg, capi.GexsLaunchCfg):
         return C.byref(cfg)
     b, w, c = cfg[:3]
-    return C.byref(capi.GexsLaunchCfg(b, w, c, cfg[3] if len(cfg) > 3 else 0))
+    return C.byref(capi.GexsLaunchCfg(b, w, c, cfg[3] if len(cfg) > 3 else 0,
+                                      cfg[4] if len(cfg) > 4 else 0))
 
 
 class Batch:

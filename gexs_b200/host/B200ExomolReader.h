@@ -15,7 +15,13 @@
 #pragma once
 #include <string>
 #include <vector>
+#ifdef GEXS_USE_REFERENCE_STATEREADER
+/* compile inside the GEXS tree against its own Readers/StateReader.h (put
+ * Readers/ on the include path; angle brackets skip this directory) */
+#include <StateReader.h>
+#else
 #include "StateReader.h"
+#endif
 #include "../../include/gexs_b200.h"
 
 class B200ExomolReader : public StateReader {
@@ -28,7 +34,8 @@ public:
                      std::string broadeners = "", double default_gamma = 0.1,
                      double default_n = 0.1, int device = 0,
                      int broad_mode = GEXS_BROAD_DEFAULTS, bool sort_by_nu = false);
-    ~B200ExomolReader() override;
+    /* not virtual, like ~StateReader: delete a B200ExomolReader* */
+    ~B200ExomolReader();
 
     bool OpenFile(std::string pFilename) override;
     bool CloseFile() override;

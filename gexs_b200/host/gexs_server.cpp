@@ -61,6 +61,7 @@ struct Req {
 struct Batch {
     cudaEvent_t ev = nullptr;
     std::vector<Req*> reqs;
+    int slot = -1;                     /* error word of this batch's kernels */
 };
 
 constexpr int kMaxBatchTemps = 1024;
@@ -78,6 +79,12 @@ struct gexs_server {
     double *d_betas = nullptr, *d_partial = nullptr, *d_q = nullptr;
     int part_chunks = 0;
     int nsm = 148;
+    /* one kernel error word per running batch (a running batch holds at
+     * least one admitted request, so max_inflight slots suffice), read
+     * back into pinned host memory behind the batch's kernels */
+    int* d_errs = nullptr;
+    int* h_errs = nullptr;
+    std::vector<int> free_slots;
 
     std::vector<List> lists;
     size_t resident = 0;
@@ -170,7 +177,21 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
         }
     }
     Batch b;
-    if (!status) status = gexs_run(s->ctx, jobs.data(), (int)jobs.size(), nullptr, (void*)st);
+    if (!status) {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (s->free_slots.empty()) {
+            status = gexs::set_error(GEXS_ERR_INVALID, "server: no free error slot");
+        } else {
+            b.slot = s->free_slots.back();
+            s->free_slots.pop_back();
+        }
+    }
+    int* d_err = status ? nullptr : s->d_errs + b.slot;
+    if (!status && gexs::zero_ints(d_err, 1, st) != cudaSuccess) status = GEXS_ERR_CUDA;
+    if (!status) status = gexs::run_jobs(s->ctx, jobs.data(), (int)jobs.size(), nullptr, (void*)st, d_err);
+    if (!status && cudaMemcpyAsync(s->h_errs + b.slot, d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                   st) != cudaSuccess)
+        status = GEXS_ERR_CUDA;
     if (!status && cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming) != cudaSuccess)
         status = GEXS_ERR_CUDA;
     if (!status && cudaEventRecord(b.ev, st) != cudaSuccess) status = GEXS_ERR_CUDA;
@@ -188,7 +209,11 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
         }
     }
     if (status) {
+        /* nothing of this batch is read back: wait for its work before the
+         * slot and the outputs are reused */
+        cudaStreamSynchronize(st);
         if (b.ev) cudaEventDestroy(b.ev);
+        if (b.slot >= 0) s->free_slots.push_back(b.slot);
         for (Req* r : adm)
             if (r->d_out) { cudaFreeAsync(r->d_out, st); r->d_out = nullptr; }
         s->cv_done.notify_all();
@@ -212,13 +237,19 @@ void worker_loop(gexs_server* s)
             cudaError_t q = cudaEventQuery(s->running[i].ev);
             if (q == cudaErrorNotReady) { ++i; continue; }
             double t = s->now_ms();
+            /* the batch's kernels flagged an error (a bounded wait ran out):
+             * its outputs are incomplete */
+            const int slot = s->running[i].slot;
+            const int kerr = (q == cudaSuccess) ? s->h_errs[slot] : 0;
             for (Req* r : s->running[i].reqs) {
-                r->state = (q == cudaSuccess) ? RQ_DONE : RQ_FAILED;
+                r->state = (q == cudaSuccess && !kerr) ? RQ_DONE : RQ_FAILED;
                 if (q != cudaSuccess) r->status = GEXS_ERR_CUDA;
+                else if (kerr) r->status = GEXS_ERR_KERNEL;
                 r->info.done_ms = t;
                 r->info.status = r->status;
                 s->n_completed++;
             }
+            s->free_slots.push_back(slot);
             /* the event is destroyed when its last request is fetched */
             s->running.erase(s->running.begin() + i);
             s->cv_done.notify_all();
@@ -298,7 +329,10 @@ int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int stre
     s->part_chunks = s->nsm * 2;
     bool ok = cudaMalloc(&s->d_betas, sizeof(double) * kMaxBatchTemps) == cudaSuccess &&
               cudaMalloc(&s->d_partial, sizeof(double) * kMaxBatchTemps * s->part_chunks) == cudaSuccess &&
-              cudaMalloc(&s->d_q, sizeof(double) * kMaxBatchTemps) == cudaSuccess;
+              cudaMalloc(&s->d_q, sizeof(double) * kMaxBatchTemps) == cudaSuccess &&
+              cudaMalloc(&s->d_errs, sizeof(int) * s->max_inflight) == cudaSuccess &&
+              cudaMallocHost(&s->h_errs, sizeof(int) * s->max_inflight) == cudaSuccess;
+    for (int i = s->max_inflight - 1; ok && i >= 0; --i) s->free_slots.push_back(i);
     if (!ok) { gexs_server_destroy(s); return gexs::set_error(GEXS_ERR_OOM, "server buffers"); }
     s->worker = std::thread(worker_loop, s);
     *out = s;
@@ -330,6 +364,8 @@ int gexs_server_destroy(gexs_server* s)
     for (cudaStream_t c : s->copy_free) cudaStreamDestroy(c);
     if (s->part_stream) cudaStreamDestroy(s->part_stream);
     cudaFree(s->d_betas); cudaFree(s->d_partial); cudaFree(s->d_q);
+    cudaFree(s->d_errs);
+    if (s->h_errs) cudaFreeHost(s->h_errs);
     gexs_ctx_destroy(s->ctx);
     delete s;
     return GEXS_OK;

@@ -154,6 +154,10 @@ typedef struct gexs_launch_cfg {
     int32_t warps;           /* 4 or 8 (tile = 32*bins*warps)        */
     int32_t ctas_per_sm;     /* resident CTAs per SM (0 = max)       */
     int32_t flags;           /* GEXS_LAUNCH_*                        */
+    int32_t wait_spins;      /* attempts of each bounded wait of the FP32
+                                Voigt pipeline before it gives up and
+                                flags GEXS_ERR_KERNEL (0 = 2^21, about
+                                0.5 s of back-off per wait)           */
 } gexs_launch_cfg;
 
 /* derive S(T), width and y of every line in the tile loader instead of
@@ -179,7 +183,12 @@ int         gexs_version(void);
 int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
              const gexs_launch_cfg* cfg, void* stream);
 
-/* Synchronise `stream` and read the context's kernel error flag. */
+/* Synchronise `stream`, then read and clear the context's kernel error
+ * word: GEXS_ERR_KERNEL if a kernel of an earlier gexs_run on this context
+ * flagged an error (a bounded wait that ran out, GEXS_KERR_* bits in the
+ * message) since the last check, else GEXS_OK.  The word is shared by
+ * every stream of the context; the read and the clear are one atomic
+ * exchange on the device, so no flag raised meanwhile is lost. */
 int gexs_ctx_check(gexs_ctx* ctx, void* stream);
 
 /* Exact number of (line, bin) profile evaluations of each job (the window
@@ -204,14 +213,31 @@ int gexs_count_evals(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
  *    device looks up the array's device address (cudaGetSymbolAddress);
  *    make that first call before any stream capture on that device.
  *  - Every call on a device shares the one array and it keeps the last
- *    call's contents (the work counter is reset by each call): calls whose
- *    work overlaps on the GPU, from any stream or thread, race and must be
- *    serialised by the caller.
- * cfg NULL = 4 bins per lane, 8 warps. */
+ *    call's contents (each call resets the work counter and the error
+ *    word): calls whose work overlaps on the GPU, from any stream or
+ *    thread, race and must be serialised by the caller.
+ *  - Lines are derived as they are loaded (no 24-byte-per-line prep
+ *    arrays) and tiles are never cut into line slices (their tables grow
+ *    with the grid), so a dense band, where a few tiles hold most of the
+ *    lines, runs on fewer SMs than with gexs_run: up to several times
+ *    slower there; elsewhere the two run alike.
+ *  - Kernel errors (a bounded wait that ran out) are not returned by this
+ *    call, which does not wait for the kernels: read them with
+ *    gexs_noalloc_status after the call.
+ * cfg NULL = gexs_run's default shape (4 bins per lane; 4 warps for FP32,
+ * 8 for FP64). */
 #define GEXS_NOALLOC_MAX_JOBS      64
 #define GEXS_NOALLOC_SCRATCH_BYTES 16384
 int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
                      void* stream);
+/* Synchronise `stream` and read the error word of the last
+ * gexs_run_noalloc on the current device into *flags (GEXS_KERR_* bits):
+ * GEXS_OK when it is zero, GEXS_ERR_KERNEL when a kernel flagged an error.
+ * A copy of four bytes to the host; allocates nothing.  The word is
+ * cleared by the next gexs_run_noalloc, not by this call. */
+#define GEXS_KERR_PIPELINE 1   /* a bounded wait of the FP32 Voigt pipeline ran out */
+#define GEXS_KERR_SLICES   2   /* line-slice tables overflowed (gexs_run only)      */
+int gexs_noalloc_status(void* stream, int* flags);
 
 /* --------------------------------------------------------- ExoMol ingest
  * The reader layer of the reference (Readers/Exomol/ExomolStateReader.cpp,

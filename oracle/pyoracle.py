@@ -20,15 +20,19 @@ _refs = {}
 
 
 def build(with_reference=None):
-    """Build the oracle (and oracle/_ref when the reference tree exists)."""
+    """Build the oracle (and oracle/_ref when the reference tree exists).
+    The tree is the Makefile's REF, or the GEXS_REFERENCE environment
+    variable when it is set."""
     import subprocess
-    ref = os.environ.get("GEXS_REFERENCE", "/root/reference")
+    ref = os.environ.get("GEXS_REFERENCE")
+    var = ["REF=" + ref] if ref else []
     targets = ["oracle"]
     if with_reference is None:
-        with_reference = os.path.isdir(ref)
+        with_reference = subprocess.run(["make", "-s", "-C", HERE] + var + ["has-ref"],
+                                        capture_output=True).returncode == 0
     if with_reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, "REF=" + ref] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE] + var + targets, check=True)
 
 
 def orc():
