@@ -423,12 +423,21 @@ def batch64(ctx, torch, dev):
 
 
 def serve_bench(torch, dev, local_rank, args):
-    """Request loop under Poisson arrivals: three resident synthetic lists
-    (1e7, 1e8, 5e8 lines; 18, 16, 44 amu), requests with T log-uniform
-    100-3000 K, P log-uniform 1e-6-100 bar, resolution log-uniform
-    0.001-0.1 cm^-1, 1e4-1e7 points inside 100-20000 cm^-1, Doppler or
-    Voigt (FP32 form).  Rates are set relative to the measured mean service
-    time; latency = result in the caller's buffer minus submission."""
+    """Request loop under Poisson arrivals (continuous batching).
+
+    Three resident synthetic lists of 1e7, 1e8 and 5e8 lines times
+    --serve-scale (18, 16, 44 amu; generated as the 1e8-line workload, the
+    largest from 1e6 states J 0-120).  One seeded set of --serve-requests
+    requests is used for every rate: list uniform, T log-U(100, 3000) K, P
+    log-U(1e-6, 100) bar, dnu log-U(0.001, 0.1) cm^-1, 1e4-1e7 points (at
+    most the span 100-20000 allows), start uniform in 100-20000 minus the
+    span, Doppler or Voigt, FP32 form.  The set is first run one request at
+    a time; its mean service time s sets the rate of offered load L as L/s.
+    Per rate the same set arrives as a Poisson stream; each request has its
+    own waiter, so a result is fetched as soon as it is done.  latency =
+    result copied into the caller's buffer minus submission (device done
+    minus submission also given); throughput = requests / (last fetch -
+    first submission)."""
     import threading
     from gexs_b200 import synth, _capi as capi
     from gexs_b200.engine import Server, Context, Job, LineList
@@ -438,7 +447,7 @@ def serve_bench(torch, dev, local_rank, args):
     keep, lists = [], []
     t_gen = time.perf_counter()
     for n, mass, k in specs:
-        big = n >= int(5e8 * scale)
+        big = k == 3
         st = synth.make_states(1000000 if big else 200000, 120 if big else 80, 1010 + k)
         L = synth.make_lines_torch(st, n, NU0, NU1, 2010 + k, broadening_seed=3010 + k, device=dev)
         lid = srv.add_list(L, st.energy, st.g, mass)
@@ -461,72 +470,79 @@ def serve_bench(torch, dev, local_rank, args):
         return li, Server.request(lists[li][0], prof, T, P, nu0, d, G, precision=capi.FP32,
                                   cutoff=CUT)
 
-    def run(reqs, rate):
-        lat, infos = [None] * len(reqs), [None] * len(reqs)
-        tickets = [None] * len(reqs)
-        ready = [threading.Event() for _ in reqs]
+    reqs = [draw() for _ in range(args.serve_requests)]
 
-        def client():
-            r2 = np.random.Generator(np.random.PCG64(4100))
-            for i, (_, rq) in enumerate(reqs):
-                if rate:
-                    time.sleep(float(r2.exponential(1.0 / rate)))
-                tickets[i] = srv.submit(rq)
-                ready[i].set()
-        th = threading.Thread(target=client)
+    def run(rate, seed):
+        n = len(reqs)
+        lat, dlat, infos = [0.0] * n, [0.0] * n, [None] * n
+        errors = []
+
+        def waiter(i, ticket, G):
+            try:
+                _, info = srv.wait(ticket, G)
+                lat[i] = info.fetched_ms - info.submit_ms
+                dlat[i] = info.done_ms - info.submit_ms
+                infos[i] = info
+            except Exception as e:  # pragma: no cover
+                errors.append(str(e))
+        r2 = np.random.Generator(np.random.PCG64(seed))
+        gaps = r2.exponential(1.0 / rate, n) if rate else np.zeros(n)
+        threads = []
         t0 = time.perf_counter()
-        th.start()
+        due = t0
         for i, (_, rq) in enumerate(reqs):
-            ready[i].wait()
-            out, info = srv.wait(tickets[i], rq.grid_points)
-            lat[i] = info.fetched_ms - info.submit_ms
-            infos[i] = info
-        th.join()
-        return time.perf_counter() - t0, lat, infos
+            due += float(gaps[i])
+            dt = due - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            th = threading.Thread(target=waiter, args=(i, srv.submit(rq), rq.grid_points))
+            th.start()
+            threads.append(th)
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        if errors:
+            raise RuntimeError(errors[0])
+        return wall, np.array(lat), np.array(dlat), infos
 
-    ctx = Context(local_rank)
-
-    def evals_of(reqs):
-        tot = 0
-        for li, rq in reqs:
-            j = Job(keep[li], torch.empty(1, dtype=torch.float64, device=dev),
-                    convention=capi.CONV_PHYSICAL, profile=rq.profile,
-                    temperature=rq.temperature, pressure=rq.pressure, partition=1.0,
-                    mass=lists[li][1], nu_start=rq.nu_start, dnu=rq.dnu,
-                    grid_points=rq.grid_points, cutoff=CUT, n_points=rq.grid_points)
-            tot += ctx.count_evals([j])[0]
-        return tot
-
-    warm = [draw() for _ in range(3)]
-    run(warm, 0.0)
-    calib = [draw() for _ in range(8)]
-    wall, lat, _ = run([(li, rq) for li, rq in calib], 0.0)
-    # serial service time: run them one by one
-    t0 = time.perf_counter()
-    for li, rq in calib:
+    # warm-up (module loads, pools), then the set one request at a time
+    for _, rq in reqs[:3]:
         srv.wait(srv.submit(rq), rq.grid_points)
-    service = (time.perf_counter() - t0) / len(calib)
+    t0 = time.perf_counter()
+    for _, rq in reqs:
+        srv.wait(srv.submit(rq), rq.grid_points)
+    service = (time.perf_counter() - t0) / len(reqs)
+    ctx = Context(local_rank)
+    ev = 0
+    for li, rq in reqs:
+        j = Job(keep[li], torch.empty(1, dtype=torch.float64, device=dev),
+                convention=capi.CONV_PHYSICAL, profile=rq.profile, temperature=rq.temperature,
+                pressure=rq.pressure, partition=1.0, mass=lists[li][1], nu_start=rq.nu_start,
+                dnu=rq.dnu, grid_points=rq.grid_points, cutoff=CUT, n_points=rq.grid_points)
+        ev += ctx.count_evals([j])[0]
     rates = []
-    for load in args.serve_loads:
-        reqs = [draw() for _ in range(args.serve_requests)]
+    for k, load in enumerate(args.serve_loads):
         rate = load / service
-        wall, lat, infos = run(reqs, rate)
-        ev = evals_of(reqs)
-        lat = np.array(lat)
-        rates.append({"offered_load": load, "rate_per_s": rate, "requests": len(reqs),
+        wall, lat, dlat, infos = run(rate, 4100 + k)
+        rates.append({"offered_load": load, "offered_req_per_s": rate, "requests": len(reqs),
                       "p50_ms": float(np.percentile(lat, 50)),
                       "p99_ms": float(np.percentile(lat, 99)),
-                      "mean_ms": float(lat.mean()), "throughput_req_per_s": len(reqs) / wall,
-                      "evals_per_s": ev / wall,
+                      "mean_ms": float(lat.mean()),
+                      "device_done_p50_ms": float(np.percentile(dlat, 50)),
+                      "device_done_p99_ms": float(np.percentile(dlat, 99)),
+                      "throughput_req_per_s": len(reqs) / wall, "evals_per_s": ev / wall,
                       "mean_batch": float(np.mean([i.batch_size for i in infos])),
                       "max_batch": int(max(i.batch_size for i in infos))})
     stats = srv.stats()
     srv.close()
     return {"lists": [{"lines": n, "mass_amu": m} for _, m, n in lists],
-            "list_generation_s": t_gen, "serial_service_ms": 1e3 * service,
+            "list_scale": scale, "list_generation_s": t_gen,
+            "serial_service_ms": 1e3 * service, "evals_per_request_set": ev,
             "rates": rates, "batches": stats["batches"],
-            "requests": "T log-U(100,3000) K, P log-U(1e-6,100) bar, dnu log-U(0.001,0.1), "
-                        "1e4-1e7 points in 100-20000 cm^-1, Doppler|Voigt, FP32 form"}
+            "requests": "one seeded set of %d for every rate: T log-U(100,3000) K, P "
+                        "log-U(1e-6,100) bar, dnu log-U(0.001,0.1), 1e4-1e7 points in "
+                        "100-20000 cm^-1, Doppler|Voigt, FP32 form" % len(reqs),
+            "latency": "result in the caller's buffer minus submission; one waiter per request"}
 
 
 def quad_suite(args):
@@ -864,17 +880,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the reference legs (CPU sample, reference GPU kernel)")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest"],
+    ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest", "serve"],
                     help="quad: Gauss-Hermite 16/32 vs Humlicek on the 5e8-line list; "
                          "ingest: ExoMol text parsed on the GPU vs the reference reader")
     ap.add_argument("--ingest-lines", type=int, default=20_000_000)
     ap.add_argument("--quad-lines", type=int, default=500_000_000)
     ap.add_argument("--shard", default="replica", choices=["replica", "grid"],
                     help="N>1: one cross-section per rank (weak) or slices of one (strong)")
-    ap.add_argument("--serve-scale", type=float, default=1.0,
+    ap.add_argument("--serve-scale", type=float, default=0.1,
                     help="scale of the three resident line lists (1 = 1e7, 1e8, 5e8 lines)")
-    ap.add_argument("--serve-requests", type=int, default=30)
-    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.9, 1.5])
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.3, 0.6, 0.9, 1.2])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--cfg", default="4,4,0",
                     help="launch shape bins_per_lane,warps,ctas_per_sm of the timed kernel")
@@ -886,6 +902,12 @@ def main():
         return reference_arm(args)
     if args.suite == "ingest":
         print(json.dumps(ingest_suite(args)), flush=True)
+        return 0
+    if args.suite == "serve":
+        import torch
+        torch.cuda.set_device(0)
+        r = serve_bench(torch, "cuda:0", 0, args)
+        print(json.dumps({"suite": "serve", **r}), flush=True)
         return 0
     if args.suite == "quad":
         r = quad_suite(args)

@@ -121,6 +121,8 @@ SIGNATURES = [
                                    C.POINTER(GexsLineTable)]),
     ("gexs_hitran_parse", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_double, C.c_double,
                                     C.c_double, C.c_int, C.POINTER(GexsLineTable)]),
+    ("gexs_tips_2011", C.c_int, [C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]),
     ("gexs_state_table_export", C.c_int, [C.POINTER(GexsStateTable)] + [C.c_void_p] * 3),
     ("gexs_line_table_export", C.c_int, [C.POINTER(GexsLineTable)] + [C.c_void_p] * 6),
     ("gexs_state_table_free", C.c_int, [C.POINTER(GexsStateTable)]),
@@ -140,6 +142,11 @@ SIGNATURES = [
     ("gexs_manager_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
                                       C.POINTER(C.c_void_p)]),
     ("gexs_manager_destroy", C.c_int, [C.c_void_p]),
+    ("gexs_manager_create_multi", C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                            C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("gexs_shard_plan", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_int64,
+                                  C.c_int64, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
     ("gexs_manager_initialize_vectors", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("gexs_manager_initialize_constants", C.c_int, [C.c_void_p] + [C.c_double] * 8),
     ("gexs_manager_transfer_freq", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -160,6 +167,8 @@ SIGNATURES = [
                                    C.POINTER(GexsRequestInfo)]),
     ("gexs_server_poll", C.c_int, [C.c_void_p, C.c_uint64]),
     ("gexs_server_stats", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 4),
+    ("gexs_server_partition", C.c_int, [C.c_void_p, C.c_int, C.c_double,
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]),
 ]
 
 _lib = None

@@ -31,6 +31,9 @@ SOURCES = [
     "host/gexs_server.cpp",
     "host/B200ExomolReader.cpp",
     "host/gexs_output.cpp",
+    "host/gexs_tips.cpp",
+    "host/gexs_shard.cpp",
+    "host/B200MultiManager.cpp",
 ]
 LIB = os.path.join(HERE, "libgexs_b200.so")
 

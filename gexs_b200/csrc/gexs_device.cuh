@@ -187,6 +187,46 @@ __device__ __forceinline__ float gh_sum_f32(float x, float y2)
     return acc;
 }
 
+/* Lines much narrower than a node spacing (y < 1/8): near a node t_k the
+ * term w_k / (y^2 + (x - t_k)^2) is a spike of width y, and an x carried
+ * in one float (absolute error ~1e-7 x) would put a relative error of
+ * about 1e-7 x / |x - t_k| on it.  Here x is the unevaluated pair xs + xl
+ * (x_pair below, error ~1e-13) and x - t_k is taken against the node split
+ * the same way, so every difference keeps its relative accuracy. */
+template <int NODES>
+__device__ __forceinline__ float gh_sum_f32_pair(float xs, float xl, float y2)
+{
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < GH<NODES>::NP; ++k) {
+        const double tk = gh_t<NODES>(k);
+        const float th = (float)tk, tl = (float)(tk - (double)th), w = (float)gh_w<NODES>(k);
+        /* xs - th is exact when xs is within a factor 2 of th (Sterbenz) */
+        const float d1 = __fadd_rn(__fsub_rn(xs, th), __fsub_rn(xl, tl));
+        const float d2 = __fadd_rn(xs, th);
+        const float A = fmaf(d1, d1, y2), B = fmaf(d2, d2, y2);
+        acc = fmaf(w * (A + B), rcp_approx(A * B), acc);
+    }
+    return acc;
+}
+
+/* x = (n - fc) dx as the pair xs + xl from n (an exact integer in float),
+ * dx = dxh + dxl and mf = -fc dx = mfh + mfl (each split from FP64 on the
+ * host of the record): TwoProduct of n dxh and TwoSum with mfh, written
+ * with _rn intrinsics so that no step is contracted into an FMA. */
+__device__ __forceinline__ void x_pair(float n, float dxh, float dxl, float mfh, float mfl,
+                                       float& xs, float& xl)
+{
+    const float p = __fmul_rn(n, dxh);
+    const float e1 = __fmaf_rn(n, dxh, -p);
+    const float s = __fadd_rn(p, mfh);
+    const float bb = __fsub_rn(s, p);
+    const float e2 = __fadd_rn(__fsub_rn(p, __fsub_rn(s, bb)), __fsub_rn(mfh, bb));
+    const float lo = __fadd_rn(__fadd_rn(e1, e2), __fmaf_rn(n, dxl, mfl));
+    /* |x|: the profile is even in x */
+    if (s < 0.f) { xs = -s; xl = -lo; } else { xs = s; xl = lo; }
+}
+
 /* same sum as 1/A + 1/B per pair: no A*B product, safe for |x| > 1e9 */
 template <int NODES>
 __device__ __forceinline__ float gh_sum_f32_wide(float x, float y2)

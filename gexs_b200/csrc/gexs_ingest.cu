@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -791,6 +792,17 @@ int gexs_hitran_parse(gexs_ctx* ctx, const char* h_text, int64_t nbytes, double 
     if (!ctx || !out || nbytes < 0 || (nbytes > 0 && !h_text))
         return set_error(GEXS_ERR_INVALID, "gexs_hitran_parse: arguments");
     std::memset(out, 0, sizeof(*out));
+    if (!(ref_partition_296 > 0.0)) {
+        /* molecule (columns 1-2) and isotopologue (column 3) of the first
+         * record by atoi of their fields (HITRANStateReader.cpp:3-39, 88-95),
+         * then TIPS-2011 at 296 K */
+        char mol[3] = {0, 0, 0}, iso[2] = {0, 0};
+        for (int k = 0; k < 2 && k < nbytes; ++k) mol[k] = h_text[k];
+        if (nbytes > 2) iso[0] = h_text[2];
+        double gi = 0.0;
+        int st = gexs_tips_2011(std::atoi(mol), std::atoi(iso), 296.0, &gi, &ref_partition_296);
+        if (st) return st;
+    }
     cudaSetDevice(ctx_device(ctx));
     cudaStream_t s = 0;
     DevBuf d_text, d_end, d_rec;

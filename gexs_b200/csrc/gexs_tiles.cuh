@@ -57,9 +57,13 @@ struct __align__(16) RecF32 {   /* 48 bytes; Doppler/Gaussian and GH */
     int   c1;              /* Doppler: bins whose xm <= the zero threshold   */
     int   mask;            /* per warp w: bit w touches, bit 8+w fast tier,
                               bit 16+w mid tier; bit 24: |x| may exceed 1e8
-                              in this tile (overflow-free forms)             */
+                              in this tile (overflow-free forms); bit 25 (GH):
+                              y < 1/8, x as a float pair (gh_sum_f32_pair)   */
     int   pad;
 };
+/* GH records reuse two fields: y holds the low part of dx and amp the low
+ * part of mfcdx (their high parts are dx and mfcdx), see make_rec */
+constexpr int GH_PAIR_BIT = 1 << 25;
 
 struct __align__(16) RecF64 {   /* 64 bytes */
     double nu;             /* centre after the nu==0 rule                   */
@@ -371,20 +375,26 @@ __device__ __forceinline__ void make_rec(RecF32& q, const Derived<PK>& d, const 
     q.mfcdx = -fc * q.dx;
     double ampd = (PK == PK_ERF) ? dmul(d.S, J.out_scale) : dmul(dmul(d.S, d.invw), J.out_scale);
     q.amp = (float)ampd;
+    bool pair = false;
     if constexpr (PK == PK_ERF) {
         q.a1 = 0.f; q.p = 0.f;
         q.y = (float)(0.5 * dx);
     } else {
         q.a1 = (float)(ampd * d.y * GEXS_INV_PI);
         q.p = (float)(d.y * d.y);
-        q.y = (float)d.y;
+        /* dx and mf = -(tc - ic) dx as (high, low) float pairs from FP64 */
+        const double mf = -(d.tc - ic) * dx;
+        q.mfcdx = (float)mf;
+        q.y = (float)(dx - (double)q.dx);
+        q.amp = (float)(mf - (double)q.mfcdx);
+        pair = d.y < 0.125;
     }
     q.fc = fc;
     q.win = d.win; q.c1 = d.c1;
     /* largest |x| the line reaches in this tile */
     double dfar = fmax(fabs(d.nu - T.f0), fabs(d.nu - T.fl));
     const int wide = (dfar * d.invw > 1e8) ? 1 : 0;
-    q.mask = (d.win == 0) ? 0 : warp_mask<PK, B, WARPS>(d, wide);
+    q.mask = (d.win == 0) ? 0 : (warp_mask<PK, B, WARPS>(d, wide) | (pair && !wide ? GH_PAIR_BIT : 0));
     q.pad = 0;
 }
 
@@ -501,6 +511,21 @@ __device__ __forceinline__ void lines_f32(const RecF32* __restrict__ rec, int nr
             }
         } else {
             constexpr int NODES = (PK == PK_GH16) ? 16 : 32;
+            if (mask & GH_PAIR_BIT) {
+                /* narrow line: x as a float pair, per-bin window test */
+                const int a = lo16(qi.x), b = hi16(qi.x);
+                const float t0 = lanef + ncf;
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = wb + lane + 32 * k;
+                    if (t < a || t >= b) continue;
+                    float xs, xl;
+                    x_pair(t0 + (float)(32 * k), q0.y, q1.y, q0.z, q1.z, xs, xl);
+                    float& acc = bin_acc<B>(part, k);
+                    acc = fmaf(q0.w, gh_sum_f32_pair<NODES>(xs, xl, q1.x), acc);
+                }
+                continue;
+            }
             if (mask & (bit << 8)) {
                 const float x0 = fmaf(lanef, q0.y, fmaf(ncf, q0.y, q0.z));
 #pragma unroll

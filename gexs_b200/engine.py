@@ -264,8 +264,16 @@ class Manager:
     host numpy arrays in and out, exactly as BaseProfile passes them."""
 
     def __init__(self, profile, device=0, convention=capi.CONV_REF_GPU, precision=capi.FP64,
-                 memory_bytes=0):
+                 memory_bytes=0, devices=None):
+        """devices (a list) makes the multi-GPU manager, one bin range per
+        entry (gexs_manager_create_multi); otherwise one device."""
         self.h = C.c_void_p()
+        if devices is not None:
+            arr = (C.c_int * len(devices))(*devices)
+            check(lib().gexs_manager_create_multi(profile, arr, len(devices), convention,
+                                                  precision, memory_bytes, C.byref(self.h)),
+                  "gexs_manager_create_multi")
+            return
         check(lib().gexs_manager_create(profile, device, convention, precision, memory_bytes,
                                         C.byref(self.h)), "gexs_manager_create")
 
@@ -397,6 +405,13 @@ class Server:
 
     def poll(self, ticket):
         return lib().gexs_server_poll(self.h, ticket)
+
+    def partition(self, list_id, temperature):
+        """(Q(T), True when it came from the resident table)"""
+        q, tab = C.c_double(), C.c_int()
+        check(lib().gexs_server_partition(self.h, list_id, temperature, C.byref(q), C.byref(tab)),
+              "gexs_server_partition")
+        return q.value, bool(tab.value)
 
     def stats(self):
         v = [C.c_int64() for _ in range(4)]

@@ -329,6 +329,26 @@ void B200Manager::TransferResults(double* h_freq, double* h_intens, int N, int I
         fail(GEXS_ERR_CUDA);
 }
 
+void B200Manager::AddResultRange(double* h_intens, int lo, int hi, int I)
+{
+    if (status_) return;
+    if (I < 0 || I >= (int)d_slots_.size() || lo < 0 || hi > npoints_ || lo > hi || !h_intens) {
+        fail(GEXS_ERR_INVALID);
+        return;
+    }
+    if (flush()) return;
+    cudaSetDevice(device_);
+    int st = gexs_ctx_check(ctx_, stream_);
+    if (st) { fail(st); return; }
+    std::vector<double> tmp((size_t)(hi - lo));
+    if (hi > lo && cudaMemcpy(tmp.data(), d_slots_[I] + lo, sizeof(double) * (size_t)(hi - lo),
+                              cudaMemcpyDeviceToHost) != cudaSuccess) {
+        fail(GEXS_ERR_CUDA);
+        return;
+    }
+    for (int j = lo; j < hi; ++j) h_intens[j] += tmp[(size_t)(j - lo)];
+}
+
 void B200Manager::Cleanup()
 {
     if (ctx_) { flush(); cudaStreamSynchronize((cudaStream_t)stream_); }
@@ -350,12 +370,18 @@ bool B200Manager::ReadyForWork()
 }
 
 /* ----------------------------------------------------------- C wrappers */
-struct gexs_manager { B200Manager* m; };
+#include "B200MultiManager.h"
+
+/* one device (single) or several (multi); m is the one in use */
+struct gexs_manager {
+    BaseManager* m = nullptr;
+    B200Manager* single = nullptr;
+    B200MultiManager* multi = nullptr;
+};
 
 static int mstat(gexs_manager* h)
 {
-    int st = h->m->last_status();
-    return st;
+    return h->single ? h->single->last_status() : h->multi->last_status();
 }
 
 extern "C" {
@@ -368,9 +394,27 @@ int gexs_manager_create(int profile, int device, int convention, int precision,
     if (profile != GEXS_GAUSSIAN && profile != GEXS_DOPPLER && profile != GEXS_VOIGT &&
         profile != GEXS_VOIGT_QUAD) return GEXS_ERR_INVALID;
     gexs_manager* h = new gexs_manager();
-    h->m = new B200Manager((ProfileType)profile, device, convention, precision, memory_bytes);
-    int st = h->m->last_status();
-    if (st) { delete h->m; delete h; return st; }
+    h->single = new B200Manager((ProfileType)profile, device, convention, precision, memory_bytes);
+    h->m = h->single;
+    int st = h->single->last_status();
+    if (st) { delete h->single; delete h; return st; }
+    *out = h;
+    return GEXS_OK;
+}
+
+int gexs_manager_create_multi(int profile, const int* devices, int ndev, int convention,
+                              int precision, size_t memory_bytes, gexs_manager** out)
+{
+    if (!out || ndev < 0 || (ndev > 0 && !devices)) return GEXS_ERR_INVALID;
+    *out = nullptr;
+    if (profile != GEXS_GAUSSIAN && profile != GEXS_DOPPLER && profile != GEXS_VOIGT &&
+        profile != GEXS_VOIGT_QUAD) return GEXS_ERR_INVALID;
+    std::vector<int> devs(devices, devices + ndev);
+    gexs_manager* h = new gexs_manager();
+    h->multi = new B200MultiManager((ProfileType)profile, devs, convention, precision, memory_bytes);
+    h->m = h->multi;
+    int st = h->multi->last_status();
+    if (st) { delete h->multi; delete h; return st; }
     *out = h;
     return GEXS_OK;
 }
@@ -378,7 +422,8 @@ int gexs_manager_create(int profile, int device, int convention, int precision,
 int gexs_manager_destroy(gexs_manager* h)
 {
     if (!h) return GEXS_OK;
-    delete h->m;
+    delete h->single;
+    delete h->multi;
     delete h;
     return GEXS_OK;
 }

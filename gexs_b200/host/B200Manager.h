@@ -74,6 +74,10 @@ public:
     bool ReadyForWork();
 
     int last_status() const { return status_; }
+    /* add bins [lo, hi) of result slot I into h_intens[lo, hi) (waits for
+     * the queued work first); B200MultiManager gathers each device's bins
+     * with it */
+    void AddResultRange(double* h_intens, int lo, int hi, int I);
     int quad_nodes = 16;     /* Gauss-Hermite nodes for VOIGT_QUAD */
 
 private:

@@ -15,6 +15,7 @@
  * is released when the caller fetches it (gexs_server_wait), which frees
  * budget for the next admissions.
  */
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -35,6 +36,14 @@ namespace {
 
 enum { RQ_PENDING = 0, RQ_RUNNING = 1, RQ_DONE = 2, RQ_FAILED = 3 };
 
+/* resident Q(T) table of a list: Q at kQPoints temperatures log-spaced
+ * over [kQTmin, kQTmax], computed once on the device when the list is
+ * added; a request's Q(T) is the 4-point Lagrange interpolation of ln Q in
+ * ln T (relative error ~1e-14 on smooth state sums, checked against the
+ * exact device sum in the tests); other temperatures take the exact sum */
+constexpr int kQPoints = 4096;
+constexpr double kQTmin = 10.0, kQTmax = 10000.0;
+
 struct List {
     double *nu = nullptr, *elow = nullptr, *aif = nullptr, *gamma = nullptr, *n = nullptr;
     int32_t* gns = nullptr;
@@ -44,7 +53,34 @@ struct List {
     int64_t nstates = 0;
     double mass = 0.0;
     size_t bytes = 0;
+    double* d_qtab = nullptr;          /* Q at the table temperatures (HBM)   */
+    std::vector<double> lnq;           /* ln Q, host mirror for job setup     */
 };
+
+double qtab_lnt(int k)
+{
+    return std::log(kQTmin) + (std::log(kQTmax) - std::log(kQTmin)) * (double)k / (kQPoints - 1);
+}
+
+/* Q(T) from the resident table; false outside its range */
+bool q_from_table(const List& L, double T, double* q)
+{
+    if (L.lnq.empty() || !(T >= kQTmin && T <= kQTmax)) return false;
+    const double h = (std::log(kQTmax) - std::log(kQTmin)) / (kQPoints - 1);
+    const double u = std::log(T);
+    int i = (int)std::floor((u - std::log(kQTmin)) / h);
+    i = std::min(std::max(i, 1), kQPoints - 3);
+    double x[4], v = 0.0;
+    for (int a = 0; a < 4; ++a) x[a] = qtab_lnt(i - 1 + a);
+    for (int a = 0; a < 4; ++a) {
+        double w = 1.0;
+        for (int b = 0; b < 4; ++b)
+            if (b != a) w *= (u - x[b]) / (x[a] - x[b]);
+        v += w * L.lnq[i - 1 + a];
+    }
+    *q = std::exp(v);
+    return true;
+}
 
 struct Req {
     uint64_t id = 0;
@@ -86,8 +122,11 @@ struct gexs_server {
     int* h_errs = nullptr;
     std::vector<int> free_slots;
 
-    std::vector<List> lists;
+    /* a deque: adding a list never moves the others, which the worker
+     * reads without the lock while it launches */
+    std::deque<List> lists;
     size_t resident = 0;
+    std::mutex part_mu;           /* the partition buffers (d_betas, d_partial, d_q) */
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -117,11 +156,14 @@ namespace {
 
 size_t output_bytes(const gexs_request& r) { return (size_t)r.grid_points * sizeof(double); }
 
-/* Q(T) for the admitted requests of one list: the partition kernel on the
- * server's own stream (no device-wide synchronisation). */
-int partitions(gexs_server* s, const List& L, const std::vector<double>& temps, std::vector<double>& q)
+/* exact Q(T) by the device reduction over the list's states (partition
+ * kernel on the server's own stream, no device-wide synchronisation);
+ * d_out (device, may be NULL) also gets the values */
+int exact_partitions(gexs_server* s, const List& L, const std::vector<double>& temps,
+                     std::vector<double>& q, double* d_out = nullptr)
 {
     const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+    std::lock_guard<std::mutex> g(s->part_mu);
     q.assign(temps.size(), 0.0);
     for (size_t off = 0; off < temps.size(); off += kMaxBatchTemps) {
         int nt = (int)std::min<size_t>(kMaxBatchTemps, temps.size() - off);
@@ -132,12 +174,32 @@ int partitions(gexs_server* s, const List& L, const std::vector<double>& temps, 
         if (e == cudaSuccess)
             e = gexs::launch_partition(L.se, L.sg, L.nstates, s->d_betas, nt, s->d_partial,
                                        s->part_chunks, s->d_q, s->part_stream);
+        if (e == cudaSuccess && d_out)
+            e = cudaMemcpyAsync(d_out + off, s->d_q, sizeof(double) * nt,
+                                cudaMemcpyDeviceToDevice, s->part_stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(q.data() + off, s->d_q, sizeof(double) * nt,
                                 cudaMemcpyDeviceToHost, s->part_stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->part_stream);
         if (e != cudaSuccess) return gexs::cuda_error(e, "server partition");
     }
+    return GEXS_OK;
+}
+
+/* Q(T) for the admitted requests of one list: from the resident table;
+ * only temperatures outside it wait for an exact device reduction */
+int partitions(gexs_server* s, const List& L, const std::vector<double>& temps, std::vector<double>& q)
+{
+    q.assign(temps.size(), 0.0);
+    std::vector<double> miss_t;
+    std::vector<size_t> miss_i;
+    for (size_t i = 0; i < temps.size(); ++i)
+        if (!q_from_table(L, temps[i], &q[i])) { miss_t.push_back(temps[i]); miss_i.push_back(i); }
+    if (miss_t.empty()) return GEXS_OK;
+    std::vector<double> mq;
+    int st = exact_partitions(s, L, miss_t, mq);
+    if (st) return st;
+    for (size_t k = 0; k < miss_i.size(); ++k) q[miss_i[k]] = mq[k];
     return GEXS_OK;
 }
 
@@ -358,7 +420,7 @@ int gexs_server_destroy(gexs_server* s)
     for (Batch& b : s->running) cudaEventDestroy(b.ev);
     for (List& L : s->lists) {
         cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
-        cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.se); cudaFree(L.sg);
+        cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.se); cudaFree(L.sg); cudaFree(L.d_qtab);
     }
     for (cudaStream_t c : s->streams) cudaStreamDestroy(c);
     for (cudaStream_t c : s->copy_free) cudaStreamDestroy(c);
@@ -381,7 +443,7 @@ int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow, c
         return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_add_list: arguments");
     const bool press = gamma && n;
     size_t bytes = (size_t)count * (3 * sizeof(double) + sizeof(int32_t) + (press ? 2 * sizeof(double) : 0)) +
-                   (size_t)nstates * (sizeof(double) + sizeof(int32_t));
+                   (size_t)nstates * (sizeof(double) + sizeof(int32_t)) + kQPoints * sizeof(double);
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (s->resident + s->inflight_bytes + bytes > s->budget)
@@ -418,6 +480,24 @@ int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow, c
     cudaMemcpy(L.se, state_energy, sizeof(double) * nstates, cudaMemcpyDefault);
     cudaError_t e = cudaMemcpy(L.sg, state_g, sizeof(int32_t) * nstates, cudaMemcpyDefault);
     if (e != cudaSuccess) return gexs::cuda_error(e, "line list upload");
+    /* the resident Q(T) table */
+    if (cudaMalloc(&L.d_qtab, sizeof(double) * kQPoints) != cudaSuccess) {
+        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
+        cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n);
+        return gexs::set_error(GEXS_ERR_OOM, "Q(T) table");
+    }
+    {
+        std::vector<double> temps(kQPoints), q;
+        for (int k = 0; k < kQPoints; ++k) temps[k] = std::exp(qtab_lnt(k));
+        const int st = exact_partitions(s, L, temps, q, L.d_qtab);
+        if (st) {
+            cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
+            cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.d_qtab);
+            return st;
+        }
+        L.lnq.resize(kQPoints);
+        for (int k = 0; k < kQPoints; ++k) L.lnq[k] = std::log(q[k]);
+    }
     std::lock_guard<std::mutex> g(s->mu);
     s->lists.push_back(L);
     s->resident += bytes;
@@ -533,6 +613,29 @@ int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_
     delete r;
     s->cv_work.notify_one();
     if (status) return gexs::set_error(status, "request failed");
+    return GEXS_OK;
+}
+
+int gexs_server_partition(gexs_server* s, int list_id, double temperature, double* q,
+                          int* from_table)
+{
+    if (!s || !q || !(temperature > 0.0))
+        return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_partition: arguments");
+    const List* L = nullptr;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (list_id < 0 || list_id >= (int)s->lists.size())
+            return gexs::set_error(GEXS_ERR_INVALID, "unknown list_id");
+        L = &s->lists[list_id];
+    }
+    cudaSetDevice(s->device);
+    const bool tab = q_from_table(*L, temperature, q);
+    if (from_table) *from_table = tab ? 1 : 0;
+    if (tab) return GEXS_OK;
+    std::vector<double> t(1, temperature), v;
+    const int st = exact_partitions(s, *L, t, v);
+    if (st) return st;
+    *q = v[0];
     return GEXS_OK;
 }
 

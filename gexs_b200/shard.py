@@ -48,6 +48,23 @@ def line_range(nu_sorted, nu_start, dnu, start_idx, n_points, cutoff):
     return lo, hi
 
 
+def plan(nu_sorted, nu_start, dnu, start_idx, n_points, reach, nshards, align=4096):
+    """gexs_shard_plan (host code of the library): bin cuts (nshards + 1)
+    with about equal evaluations on multiples of `align` from start_idx,
+    and each shard's line index range [lo, hi) within `reach`."""
+    import ctypes as C
+    from . import _capi as capi
+    nu = np.ascontiguousarray(nu_sorted, dtype=np.float64)
+    b = np.zeros(nshards + 1, dtype=np.int64)
+    lo = np.zeros(nshards, dtype=np.int64)
+    hi = np.zeros(nshards, dtype=np.int64)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    capi.check(capi.lib().gexs_shard_plan(p(nu), len(nu), nu_start, dnu, start_idx, n_points,
+                                          reach, align, nshards, p(b), p(lo), p(hi)),
+               "gexs_shard_plan")
+    return b, lo, hi
+
+
 def round_robin(jobs, rank, world):
     """The jobs of one rank when (T, P) pairs are spread over ranks."""
     return [j for i, j in enumerate(jobs) if i % world == rank]

@@ -295,12 +295,25 @@ int gexs_exomol_load(gexs_ctx* ctx, const char* states_path, const char* trans_p
  * gamma_self, E'', n_air and g' by atof of their columns; gamma =
  * (gamma_air*air_mixture + gamma_self*(1-air_mixture))*pressure (:218);
  * where A == 0, A = S*8*pi*c*Q(296)*nu^2/(exp(-c2 E''/296)*(1-exp(-c2
- * nu/296))) and g' = 1 (:222-247).  Q(296) is the caller's: the reference
- * takes it from the TIPS-2011 Fortran tables (BD_TIPS_2011_v1p0.for), which
- * this library does not carry. */
+ * nu/296))) and g' = 1 (:222-247).  ref_partition_296 <= 0 takes Q(296)
+ * from TIPS-2011 (gexs_tips_2011) for the molecule and isotopologue in
+ * columns 1-2 and 3 of the first record, as the reference does (:88-95);
+ * a positive value is used as given. */
 int gexs_hitran_parse(gexs_ctx* ctx, const char* h_text, int64_t nbytes, double pressure,
                       double air_mixture, double ref_partition_296, int sort_by_nu,
                       gexs_line_table* out);
+
+/* TIPS-2011 total internal partition sum of a HITRAN molecule (HITRAN
+ * number) and isotopologue (its 1-based index in the HITRAN file) at
+ * `temperature` K: the reference's BD_TIPS_2011
+ * (Readers/HITRAN/BD_TIPS_2011_v1p0.for:5-345, called through
+ * bd_tips_2011_ at Readers/HITRAN/HITRANStateReader.cpp:62,95,128), its
+ * tables (Q at 60, 85, ..., 3010 K) interpolated by the 3/4-point Lagrange
+ * rule of its AtoB (:5830-5920).  *gi gets the state-independent
+ * degeneracy.  Outside 70-3000 K: *q = -1 and GEXS_ERR_INVALID (the
+ * reference returns -1 with a message); molecules 34 and 39: gi = 0, Q = 0
+ * and GEXS_OK, as the reference.  Host computation, no device. */
+int gexs_tips_2011(int molecule, int isotopologue, double temperature, double* gi, double* q);
 
 /* copy a table into caller-owned device arrays of `count` elements */
 int gexs_state_table_export(const gexs_state_table* t, double* d_energy, int32_t* d_g,
@@ -356,6 +369,21 @@ int gexs_partition(gexs_ctx* ctx, const double* d_energy, const int32_t* d_g,
                    int64_t nstates, const double* h_temps, int nt,
                    double* h_q);
 
+/* ------------------------------------------------------------ sharding
+ * Split bins [start_idx, start_idx + n_points) of a grid (nu_start, dnu)
+ * into nshards ranges bounds[r] .. bounds[r+1] (nshards + 1 entries) with
+ * about equal (line, bin) evaluations - a bin's work is the number of
+ * lines within `reach` of it, sampled every 256th bin from the sorted
+ * centres h_nu (host) - interior cuts on multiples of `align` bins from
+ * start_idx (4096 makes every shard's tiles the tiles of one unsplit
+ * launch), and give each range the index range [line_lo[r], line_hi[r]) of
+ * the lines within `reach` of it.  Host computation.  No counterpart in
+ * the reference (its multi-GPU manager splits by line chunks,
+ * Managers/Accel/GPU/MultiGPUManager.cpp:59-63). */
+int gexs_shard_plan(const double* h_nu, int64_t nlines, double nu_start, double dnu,
+                    int64_t start_idx, int64_t n_points, double reach, int align, int nshards,
+                    int64_t* bounds, int64_t* line_lo, int64_t* line_hi);
+
 /* ------------------------------------------------------------ calibration
  * Measured FP32 FMA throughput of `device` in TFLOP/s (2 FLOP per FMA):
  * the roofline denominator of the FP32-profile kernels, which are bound by
@@ -372,6 +400,17 @@ typedef struct gexs_manager gexs_manager;
 int gexs_manager_create(int profile, int device, int convention,
                         int precision, size_t memory_bytes,
                         gexs_manager** out);
+/* The same manager over several GPUs: the drop-in beside the reference's
+ * MultiGpuManager (Managers/Accel/GPU/MultiGPUManager.cpp, the manager
+ * Profiles/BaseProfile.cpp:61 creates).  Each line chunk is split by grid
+ * bins into one range per device (gexs_shard_plan), each device receives
+ * only the lines that can reach its range and computes exactly the sums a
+ * single launch computes for those bins; transfer_results adds the initial
+ * grid once and every device's bins into h_intens (the reference adds each
+ * GPU's full grid).  devices may repeat a device (several shards on one
+ * GPU); ndev 0 = every visible device.  memory_bytes is per device. */
+int gexs_manager_create_multi(int profile, const int* devices, int ndev, int convention,
+                              int precision, size_t memory_bytes, gexs_manager** out);
 int gexs_manager_destroy(gexs_manager* m);
 /* BaseManager::InitializeVectors(int Npoints, int num_cs) */
 int gexs_manager_initialize_vectors(gexs_manager* m, int npoints, int num_cs);

@@ -2,12 +2,17 @@
  * gexs_serve.h — request loop in front of the cross-section kernels.
  *
  * No counterpart in the reference, which computes one configured run per
- * process (main.cpp:17-42).  The server keeps line lists and their states
- * resident in HBM, computes Q(T) on the device for each request
- * (gexs_partition), admits requests while their output grids fit in the
- * memory budget, and launches every group of newly admitted requests as one
- * persistent launch on one of several streams, so requests that arrive
- * while others run overlap with them on the device (continuous batching).
+ * process (main.cpp:17-42).  The server keeps line lists, their states and
+ * a Q(T) table per list resident in HBM, admits requests while their output
+ * grids fit in the memory budget, and launches every group of newly
+ * admitted requests as one persistent launch on one of several streams, so
+ * requests that arrive while others run overlap with them on the device
+ * (continuous batching).  The Q(T) table holds the device sum over the
+ * list's states (as gexs_partition) at 4096 temperatures log-spaced over
+ * 10-10000 K, computed when the list is added; a request's Q(T) is the
+ * 4-point Lagrange interpolation of ln Q in ln T (relative error ~1e-14 on
+ * smooth state sums), so admission never waits for a reduction; a
+ * temperature outside the table takes the exact device sum.
  * Each request's bins sum their lines in the same order whatever it is
  * batched with, so a result is bit-identical alone and in a mix.
  *
@@ -90,6 +95,12 @@ int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_
 
 /* GEXS_OK when the request's result is ready, GEXS_ERR_NOT_READY if not. */
 int gexs_server_poll(gexs_server* s, uint64_t ticket);
+
+/* Q(T) of a list as the server uses it: *from_table = 1 when it comes from
+ * the resident table, 0 when it is the exact device sum (temperature
+ * outside the table). */
+int gexs_server_partition(gexs_server* s, int list_id, double temperature, double* q,
+                          int* from_table);
 
 /* Counters: submitted, completed, admitted batches, bytes in flight. */
 int gexs_server_stats(gexs_server* s, int64_t* submitted, int64_t* completed,

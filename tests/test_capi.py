@@ -85,3 +85,5 @@ def test_bad_arguments_are_rejected_on_cpu():
     assert L.gexs_batch_launch(None, None) == -1
     assert L.gexs_manager_execute(None, 1, 1, 0, 1.0, 1.0, 1.0) == -1
     assert L.gexs_server_submit(None, None, None) == -1
+    assert L.gexs_manager_create_multi(capi.VOIGT, None, 1, 0, 0, 0, None) == -1
+    assert L.gexs_shard_plan(None, 5, 0.0, 1.0, 0, 10, 1.0, 4096, 2, None, None, None) == -1

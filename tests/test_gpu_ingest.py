@@ -174,3 +174,38 @@ def test_hitran_matches_oracle(gpu_ctx, sort):
     assert _bits_equal(a[~rebuilt], b[~rebuilt])
     ulp = np.spacing(np.abs(b[rebuilt]))
     assert (np.abs(a[rebuilt] - b[rebuilt]) <= 4 * ulp).all()
+
+
+def test_hitran_cross_section_at_1000_K_with_tips(gpu_ctx):
+    """The synthetic .par file is H2O 161 (molecule 1, isotopologue 1).
+    ref_partition_296 = 0 makes gexs_hitran_parse take Q(296) for the A it
+    rebuilds from S from TIPS-2011, as the reference does
+    (HITRANStateReader.cpp:88-95); Q(1000 K) for S(T) comes from
+    gexs_tips_2011 too (:128).  Lines against the oracle's parse with the
+    same Q(296) (A rebuilt within 4 ulp), then the FP64 Voigt cross-section
+    at 1000 K against the FP64 oracle within 1e-10 per bin."""
+    import ctypes as C
+    from gexs_b200.engine import parse_hitran
+    gi, q296, q1000 = C.c_double(), C.c_double(), C.c_double()
+    capi.check(capi.lib().gexs_tips_2011(1, 1, 296.0, C.byref(gi), C.byref(q296)), "tips")
+    capi.check(capi.lib().gexs_tips_2011(1, 1, 1000.0, C.byref(gi), C.byref(q1000)), "tips")
+    assert 170.0 < q296.value < 180.0 and q1000.value > q296.value
+    text = synth.make_hitran_par(20000, 93)
+    got = parse_hitran(gpu_ctx, text, pressure=1.0, air_mixture=0.7, ref_partition_296=0.0,
+                       sort_by_nu=True)
+    ref = po.hitran(text, 1.0, 0.7, q296.value, sort_by_nu=True)
+    a, b = got["aif"].cpu().numpy(), ref["aif"]
+    assert (np.abs(a - b) <= 4 * np.spacing(np.abs(b))).all()
+    lines = LineList(got["nu"], got["elow"], got["aif"], got["gns"], got["gamma"], got["n"])
+    host = {k: got[k].cpu().numpy() for k in ("nu", "elow", "aif", "gns", "gamma", "n")}
+    G = 300000
+    out = torch.zeros(G, dtype=torch.float64, device="cuda")
+    j = Job(lines, out, convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=1000.0,
+            pressure=1.0, partition=q1000.value, mass=18.0, nu_start=500.0, dnu=0.025,
+            grid_points=G, precision=capi.FP64, cutoff=25.0)
+    gpu_ctx.run([j])
+    gpu_ctx.check()
+    want = H.oracle_of(j, host)
+    assert want.max() > 0
+    worst, nbad = H.fp64_mismatch(out.cpu().numpy(), want)
+    assert nbad == 0, worst

@@ -220,3 +220,13 @@ def test_prep_and_on_load_paths_agree_bitwise(gpu_ctx, small_lines, prec, profil
     gpu_ctx.run([b], cfg=(4, 8, 0, capi.LAUNCH_DERIVE_ON_LOAD))
     gpu_ctx.check()
     assert torch.equal(a.out, b.out)
+
+
+@pytest.mark.parametrize("nodes", [16, 32])
+@pytest.mark.parametrize("P", [1e-3, 1.0, 100.0])
+def test_gauss_hermite_fp32_across_pressures(gpu_ctx, small_lines, nodes, P):
+    """FP32 Gauss-Hermite against the FP64 oracle of the same quadrature
+    from narrow (y << 1, float-pair x near the nodes) to broad lines."""
+    job = _make(small_lines, capi.FP32, capi.VOIGT_QUAD, nodes, capi.CONV_PHYSICAL, T=2500.0,
+                P=P, nu0=1000.0, dnu=0.01, G=150000, cutoff=25.0)
+    _check(gpu_ctx, job, small_lines)

@@ -123,3 +123,21 @@ def test_wait_timeout_and_bad_requests(served):
     assert srv.try_submit(bad)[0] == capi.GEXS_ERR_INVALID
     no_broadening = Server.request(lid_dop, capi.VOIGT, 1500.0, 1.0, 100.0, 0.01, 1000)
     assert srv.try_submit(no_broadening)[0] == capi.GEXS_ERR_INVALID
+
+
+def test_resident_partition_table(served, small_states):
+    """Q(T) from the list's resident table (4096 temperatures over 10-10000 K,
+    4-point Lagrange in ln Q / ln T) within 1e-12 of the oracle's exact sum;
+    temperatures outside the table take the exact device sum."""
+    from oracle import pyoracle as po
+    srv, lid, _ = served
+    rng = np.random.Generator(np.random.PCG64(17))
+    for T in list(10 ** rng.uniform(1.2, 3.95, 40)) + [10.0, 10000.0, 296.0]:
+        q, tab = srv.partition(lid, float(T))
+        want = po.partition(small_states.energy, small_states.g, float(T))
+        assert tab
+        assert abs(q - want) <= 1e-12 * want, (T, q, want)
+    for T in (5.0, 20000.0):
+        q, tab = srv.partition(lid, T)
+        want = po.partition(small_states.energy, small_states.g, T)
+        assert not tab and abs(q - want) <= 1e-13 * want
