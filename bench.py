@@ -422,6 +422,79 @@ def batch64(ctx, torch, dev):
                       "0.005": int(np.sum(dnus == 0.005))}}
 
 
+def batch_north_star(ctx, torch, dev, lines, st, fpe, fp64_peak, cfg):
+    """64 (T, P) cross-sections of the 1e8-line list on the 2,990,001-bin grid
+    (T log-spaced 100-3000 K x P log-spaced 1e-5-100 bar, 0.01 cm^-1 over
+    100-30000, cutoff 25): the FP32 form as one batch (gexs_batch, lines
+    derived on load: prep arrays for 64 pairs would take 154 GB) captured in
+    a CUDA graph and replayed, timed with CUDA events on its stream; the
+    plain FP64 form one launch per pair on the 8 pairs (T_i, P_i) of the
+    diagonal, its time per evaluation scaled to the 64 pairs' evaluations,
+    with the FP32 form's error against it on those 8 pairs."""
+    from gexs_b200 import _capi as capi
+    from gexs_b200.engine import Job
+    temps = np.logspace(np.log10(100.0), np.log10(3000.0), 8)
+    press = np.logspace(-5.0, 2.0, 8)
+    qs = ctx.partition(torch.as_tensor(st.energy, device=dev),
+                       torch.as_tensor(st.g, dtype=torch.int32, device=dev), np.repeat(temps, 8))
+    G = grid_points()
+    kw = dict(convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, mass=MASS, nu_start=NU0, dnu=DNU,
+              grid_points=G, cutoff=CUT)
+    j32 = [Job(lines, torch.zeros(G, dtype=torch.float64, device=dev), precision=capi.FP32,
+               temperature=float(temps[i // 8]), pressure=float(press[i % 8]),
+               partition=float(qs[i]), **kw) for i in range(64)]
+    evals = sum(ctx.count_evals(j32))
+    bcfg = tuple(cfg[:3]) + (capi.LAUNCH_DERIVE_ON_LOAD,) + tuple(cfg[4:])
+    b = ctx.batch(j32, bcfg)
+    s = torch.cuda.Stream(device=dev)
+    b.capture(s)
+    b.replay(s)
+    s.synchronize()
+    ctx.check(s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    b.replay(s)
+    e1.record(s)
+    e1.synchronize()
+    ctx.check(s)
+    t32 = e0.elapsed_time(e1)
+    b.close()
+    diag = [i * 8 + i for i in range(8)]
+    cur = torch.cuda.current_stream(dev)
+    out64 = torch.zeros(G, dtype=torch.float64, device=dev)
+    worst, band, t64, ev64 = 0.0, 0.0, 0.0, 0
+    for n, i in enumerate(diag):
+        j = Job(lines, out64, precision=capi.FP64, temperature=float(temps[i // 8]),
+                pressure=float(press[i % 8]), partition=float(qs[i]), **kw)
+        if n == 0:
+            ctx.run([j], stream=cur)
+            ctx.check(cur)
+        e0.record(cur); ctx.run([j], stream=cur); e1.record(cur); e1.synchronize()
+        ctx.check(cur)
+        t64 += e0.elapsed_time(e1)
+        ev64 += ctx.count_evals([j])[0]
+        x, r = j32[i].out, out64
+        m = r > 1e-6 * float(r.max())
+        worst = max(worst, float(((x[m] - r[m]).abs() / r[m]).max()))
+        band = max(band, abs(float(x.sum()) - float(r.sum())) / float(r.sum()))
+    t64_all = t64 * evals / ev64
+    del j32
+    torch.cuda.empty_cache()
+    fp64_tf = fpe * ev64 / (t64 * 1e-3) / 1e12
+    return {"pairs": 64, "lines": lines.count, "grid_points": G, "evals": evals,
+            "fp32_batched_ms": t32, "fp32_evals_per_s": evals / (t32 * 1e-3),
+            "fp64_plain_ms_8_pairs": t64, "fp64_plain_ms_64_pairs_scaled": t64_all,
+            "speedup": t64_all / t32,
+            "max_rel_err_vs_fp64_8_pairs": worst, "max_band_err_vs_fp64_8_pairs": band,
+            "fp64_roofline": {"achieved_tflops": fp64_tf, "peak_tflops": fp64_peak,
+                              "frac": fp64_tf / fp64_peak if fp64_peak else None,
+                              "flop_per_eval": fpe,
+                              "peak_source": "measured FP64 FMA rate (gexs_probe_fp64_tflops)"},
+            "launch_cfg": list(bcfg),
+            "fp64_scaling": "time per evaluation of the 8 diagonal pairs times the 64 pairs' "
+                            "evaluations (every pair has the same window, so the same count)"}
+
+
 def serve_bench(torch, dev, local_rank, args):
     """Request loop under Poisson arrivals (continuous batching).
 
@@ -794,6 +867,12 @@ def our_arm(args):
         pv = C.c_double()
         if lib().gexs_probe_fp32_tflops(local_rank, C.byref(pv)) == 0:
             peak = pv.value
+        peak64 = None
+        if lib().gexs_probe_fp64_tflops(local_rank, C.byref(pv)) == 0:
+            peak64 = pv.value
+        rcp = None
+        if lib().gexs_probe_rcp_gops(local_rank, C.byref(pv)) == 0:
+            rcp = pv.value
         fpe, frac = region_flops(L, q)
         achieved = evals * fpe / (launch_ms * 1e-3) / 1e12
         line_bytes = lines.nbytes()
@@ -838,12 +917,24 @@ def our_arm(args):
                                   "(region I) + core_kernel (regions II-IV), CUDA events on "
                                   "the launching stream; per-kernel shares in the ncu launch "
                                   "list under profiles/",
-                         "line_stream_gbs": line_bytes / (launch_ms * 1e-3) / 1e9},
+                         "line_stream_gbs": line_bytes / (launch_ms * 1e-3) / 1e9,
+                         "fp64_peak_tflops": peak64,
+                         "mufu": {"rcp_gops_measured": rcp,
+                                  "region1_evals_per_s": evals * frac[0] / (launch_ms * 1e-3),
+                                  "frac": (evals * frac[0] / (launch_ms * 1e-3)) / (rcp * 1e9)
+                                          if rcp else None,
+                                  "note": "region I takes one MUFU reciprocal per evaluation; "
+                                          "frac = its evaluations/s over the measured "
+                                          "rcp.approx.f32 rate"}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "path": "gexs_manager_* C ABI, pinned host",
                     "max_abs_diff_vs_device_run_over_peak": e2e_match},
             "fp64_plain": {"ms": fp64_ms, "evals_per_s": evals / (fp64_ms * 1e-3),
-                           "fp32_speedup": fp64_ms / launch_ms},
+                           "fp32_speedup": fp64_ms / launch_ms,
+                           "roofline_frac": (evals * fpe / (fp64_ms * 1e-3) / 1e12) / peak64
+                           if peak64 else None,
+                           "roofline_note": "algorithmic FLOP per evaluation x evaluations/s "
+                                            "over the measured FP64 FMA rate"},
             "accuracy": {"fp32_max_rel_vs_fp64_bins_gt_1e-6_peak": fp32_err,
                          "fp32_band_rel_vs_fp64": band_err, "integrated_fp64": integral,
                          "vs_oracle_subband": vs_oracle},
@@ -853,6 +944,9 @@ def our_arm(args):
         result["reference_gpu_kernel"] = gpu_reference_sample(torch, ctx, L, q, dev)
     if not args.no_batch and rank == 0:
         result["batch64"] = batch64(ctx, torch, dev)
+        result["batch_64_pairs_1e8_lines"] = batch_north_star(
+            ctx, torch, dev, lines, st, result["roofline"]["flop_per_eval"],
+            result["roofline"].get("fp64_peak_tflops"), cfg)
     if not args.no_serve and rank == 0:
         del lines, job, out, L
         torch.cuda.empty_cache()

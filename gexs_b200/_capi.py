@@ -111,6 +111,8 @@ SIGNATURES = [
     ("gexs_partition", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
     ("gexs_probe_fp32_tflops", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    ("gexs_probe_fp64_tflops", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    ("gexs_probe_rcp_gops", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     ("gexs_exomol_parse_states", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64,
                                            C.POINTER(GexsStateTable)]),
     ("gexs_exomol_parse_trans", C.c_int, [C.c_void_p, C.POINTER(GexsStateTable), C.c_char_p,

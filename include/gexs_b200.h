@@ -390,6 +390,13 @@ int gexs_shard_plan(const double* h_nu, int64_t nlines, double nu_start, double 
  * FP32/SFU issue rather than HBM or tensor cores.  No reference
  * counterpart. */
 int gexs_probe_fp32_tflops(int device, double* tflops);
+/* Measured FP64 FMA throughput in TFLOP/s: the roofline denominator of the
+ * plain FP64 form.  No reference counterpart. */
+int gexs_probe_fp64_tflops(int device, double* tflops);
+/* Measured rate of rcp.approx.f32 (one MUFU reciprocal) in 1e9/s: region I
+ * of the FP32 Voigt form takes one per evaluation, so this caps its
+ * evaluations/s.  No reference counterpart. */
+int gexs_probe_rcp_gops(int device, double* gops);
 
 /* ------------------------------------------------------------ manager ABI
  * Flat C view of the drop-in manager (B200Manager, a BaseManager subclass):
