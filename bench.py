@@ -619,7 +619,8 @@ def serve_bench(torch, dev, local_rank, args):
 
 
 def quad_suite(args):
-    """Voigt-Quad against Humlicek on the 5e8-line list: 1e6 states (J 0-120),
+    """Voigt-Quad against Humlicek on the 5e8-line list (resident compact:
+    FP64 nu0, float E'', g'A, gamma, n): 1e6 states (J 0-120),
     nu0 10-20000 cm^-1, T = 2500 K, P = 1e-3, 1, 100 bar, 0.01 cm^-1 over
     10-20000 (1,999,001 points), cutoff 25, FP32 form timed per
     (P, method); errors of the FP32 form against the FP64 form of the same
@@ -633,7 +634,9 @@ def quad_suite(args):
     n = args.quad_lines
     st = synth.make_states(1000000, 120, 1004)
     L = synth.make_lines_torch(st, n, 10.0, 20000.0, 2004, broadening_seed=3004, device=dev)
-    lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev)
+    # resident as the configuration states: FP64 nu0, float E'', g'A, gamma, n (24 B/line)
+    lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev,
+                     compact=True)
     del L
     torch.cuda.empty_cache()
     T = 2500.0

@@ -25,10 +25,13 @@ ERF_STABLE, ERF_LITERAL = 0, 1
 CONV_PHYSICAL, CONV_REF_CPU, CONV_REF_GPU = 0, 1, 2
 
 
+LINES_FP64, LINES_COMPACT = 0, 1
+
+
 class GexsLines(C.Structure):
     _fields_ = [("nu", C.c_void_p), ("elow", C.c_void_p), ("aif", C.c_void_p),
                 ("gns", C.c_void_p), ("gamma", C.c_void_p), ("n", C.c_void_p),
-                ("count", C.c_int64)]
+                ("count", C.c_int64), ("format", C.c_int32), ("reserved", C.c_int32)]
 
 
 class GexsJob(C.Structure):

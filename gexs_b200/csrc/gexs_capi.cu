@@ -45,7 +45,10 @@ int validate_job(const gexs_job& j, int i)
     if (j.erf_form != GEXS_ERF_STABLE && j.erf_form != GEXS_ERF_LITERAL) return bad("erf_form");
     if (!j.out) return bad("out is NULL");
     if (j.lines.count < 0) return bad("negative line count");
-    if (j.lines.count > 0 && (!j.lines.nu || !j.lines.elow || !j.lines.aif || !j.lines.gns))
+    if (j.lines.format != GEXS_LINES_FP64 && j.lines.format != GEXS_LINES_COMPACT)
+        return bad("line format");
+    const bool compact = j.lines.format == GEXS_LINES_COMPACT;
+    if (j.lines.count > 0 && (!j.lines.nu || !j.lines.elow || !j.lines.aif || (!compact && !j.lines.gns)))
         return bad("line arrays are NULL");
     bool press = j.profile == GEXS_VOIGT || j.profile == GEXS_VOIGT_QUAD;
     if (press && j.lines.count > 0 && (!j.lines.gamma || !j.lines.n))
@@ -227,6 +230,13 @@ static std::vector<unsigned char> group_image(const Group& g, const Layout& L, u
     for (size_t i = 0; i < g.jobs.size(); ++i)
         pp[i] = prep ? reinterpret_cast<double*>(dev + L.job_prep[i]) : nullptr;
     return h;
+}
+
+static bool has_compact(const Group& g)
+{
+    for (const gexs_job& j : g.jobs)
+        if (j.lines.format == GEXS_LINES_COMPACT) return true;
+    return false;
 }
 
 static int64_t max_lines(const Group& g)
@@ -460,6 +470,7 @@ int gexs::run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_la
         const Group& g = groups[gi];
         if (g.nitems == 0) continue;
         const bool prep = !(cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
+        if (!prep && has_compact(g)) return set_error(GEXS_ERR_INVALID, "compact line lists need the prep arrays");
         Layout L = group_layout(g, prep, cfgs[gi]);
         void* d = nullptr;
         e = ctx->pool ? cudaMallocFromPoolAsync(&d, L.bytes, ctx->pool, s)
@@ -546,6 +557,10 @@ int gexs_batch_create(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const Group& g = b->groups[gi];
         const bool prep = !(b->cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
+        if (!prep && has_compact(g)) {
+            gexs_batch_destroy(b);
+            return set_error(GEXS_ERR_INVALID, "compact line lists need the prep arrays");
+        }
         Layout L = group_layout(g, prep, b->cfgs[gi]);
         void* d = nullptr;
         if (cudaMalloc(&d, L.bytes) != cudaSuccess) { gexs_batch_destroy(b); return set_error(GEXS_ERR_OOM, "batch tables"); }

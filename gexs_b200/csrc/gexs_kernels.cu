@@ -21,14 +21,28 @@ __global__ void prep_kernel(const gexs_job* __restrict__ jobs, double* const* __
     double* base = prep[blockIdx.y];
     const int64_t N = J.lines.count;
     const bool press = J.profile == GEXS_VOIGT || J.profile == GEXS_VOIGT_QUAD;
+    const bool compact = J.lines.format == GEXS_LINES_COMPACT;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
          i += (int64_t)gridDim.x * blockDim.x) {
         RawLine L;
-        L.nu = J.lines.nu[i]; L.elow = J.lines.elow[i]; L.aif = J.lines.aif[i];
-        L.g = J.lines.gns[i];
+        L.nu = J.lines.nu[i];
+        if (compact) {
+            /* floats widened to FP64; aif holds g' A */
+            L.elow = (double)reinterpret_cast<const float*>(J.lines.elow)[i];
+            L.aif = (double)reinterpret_cast<const float*>(J.lines.aif)[i];
+            L.g = 1;
+        } else {
+            L.elow = J.lines.elow[i]; L.aif = J.lines.aif[i];
+            L.g = J.lines.gns[i];
+        }
         LineQ q;
         if (press) {
-            L.gam = J.lines.gamma[i]; L.nexp = J.lines.n[i];
+            if (compact) {
+                L.gam = (double)reinterpret_cast<const float*>(J.lines.gamma)[i];
+                L.nexp = (double)reinterpret_cast<const float*>(J.lines.n)[i];
+            } else {
+                L.gam = J.lines.gamma[i]; L.nexp = J.lines.n[i];
+            }
             q = line_quantities<true>(J, L);
         } else {
             L.gam = 0.0; L.nexp = 0.0;

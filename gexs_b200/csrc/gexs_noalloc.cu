@@ -86,6 +86,8 @@ extern "C" int gexs_run_noalloc(const gexs_job* jobs, int njobs, const gexs_laun
     for (int i = 0; i < njobs; ++i) {
         int st = validate_job(jobs[i], i);
         if (st) return st;
+        if (jobs[i].lines.format != GEXS_LINES_FP64)
+            return set_error(GEXS_ERR_INVALID, "gexs_run_noalloc: compact line lists need prep arrays");
         if (profile_class(jobs[i]) != pk || jobs[i].precision != prec)
             return set_error(GEXS_ERR_INVALID,
                              "gexs_run_noalloc: all jobs of a call need one profile and precision");

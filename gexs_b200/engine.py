@@ -23,21 +23,46 @@ def _stream_handle(stream):
 
 
 class LineList:
-    """Device-resident line list (structure of arrays, sorted by nu)."""
+    """Device-resident line list (structure of arrays, sorted by nu).
 
-    def __init__(self, nu, elow, aif, gns, gamma=None, n=None, device="cuda"):
+    compact=True stores nu in FP64 and E'', g'A, gamma, n as float
+    (GEXS_LINES_COMPACT, 24 bytes per line): gns is folded into aif."""
+
+    def __init__(self, nu, elow, aif, gns, gamma=None, n=None, device="cuda", compact=False):
         import torch
         def to(a, dt):
             if a is None:
                 return None
             return torch.as_tensor(a, dtype=dt).to(device).contiguous()
+        self.compact = compact
         self.nu = to(nu, torch.float64)
-        self.elow = to(elow, torch.float64)
-        self.aif = to(aif, torch.float64)
-        self.gns = to(gns, torch.int32)
-        self.gamma = to(gamma, torch.float64)
-        self.n = to(n, torch.float64)
+        if compact:
+            ga = torch.as_tensor(aif, dtype=torch.float64).to(device) * \
+                torch.as_tensor(gns).to(device).to(torch.float64)
+            self.elow = to(elow, torch.float32)
+            self.aif = ga.to(torch.float32).contiguous()
+            self.gns = None
+            self.gamma = to(gamma, torch.float32)
+            self.n = to(n, torch.float32)
+        else:
+            self.elow = to(elow, torch.float64)
+            self.aif = to(aif, torch.float64)
+            self.gns = to(gns, torch.int32)
+            self.gamma = to(gamma, torch.float64)
+            self.n = to(n, torch.float64)
         self.count = int(self.nu.shape[0])
+
+    def widened(self):
+        """The values the kernels compute with, as FP64 host arrays (g' = 1
+        for a compact list): what the oracle is given to check it."""
+        d = {"nu": self.nu.cpu().numpy(), "elow": self.elow.double().cpu().numpy(),
+             "aif": self.aif.double().cpu().numpy()}
+        d["gns"] = (np.ones(self.count, dtype=np.int32) if self.compact
+                    else self.gns.cpu().numpy())
+        if self.gamma is not None:
+            d["gamma"] = self.gamma.double().cpu().numpy()
+            d["n"] = self.n.double().cpu().numpy()
+        return d
 
     @classmethod
     def from_dict(cls, d, device="cuda"):
@@ -45,7 +70,8 @@ class LineList:
 
     def c_lines(self):
         return capi.GexsLines(_ptr(self.nu), _ptr(self.elow), _ptr(self.aif), _ptr(self.gns),
-                              _ptr(self.gamma), _ptr(self.n), self.count)
+                              _ptr(self.gamma), _ptr(self.n), self.count,
+                              capi.LINES_COMPACT if self.compact else capi.LINES_FP64)
 
     def nbytes(self):
         return sum(t.numel() * t.element_size() for t in

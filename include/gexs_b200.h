@@ -71,7 +71,18 @@ extern "C" {
  * Structure-of-arrays, exactly the arrays BaseManager::TransferVectors
  * receives (Managers/BaseManager.h:26).  Lines must be sorted by nu
  * ascending (BaseProfile.cpp:152-155 relies on the same order).  gamma and
- * n may be NULL for profiles that do not use pressure broadening. */
+ * n may be NULL for profiles that do not use pressure broadening.
+ *
+ * format GEXS_LINES_COMPACT keeps nu in FP64 and the rest in 4 bytes:
+ * elow, aif, gamma and n point to float arrays (cast to these pointer
+ * types), aif holding the product g' * A, and gns is unused: 24 bytes per
+ * line with broadening instead of 44.  Every kernel widens the floats to
+ * FP64 and computes as for the FP64 list (g' = 1, A = g'A); the per-job
+ * prep arrays are required (GEXS_LAUNCH_DERIVE_ON_LOAD and
+ * gexs_run_noalloc reject compact lists). */
+#define GEXS_LINES_FP64    0
+#define GEXS_LINES_COMPACT 1
+
 typedef struct gexs_lines {
     const double*  nu;     /* line centre nu0 [cm^-1]                      */
     const double*  elow;   /* lower-state energy [cm^-1]                   */
@@ -80,6 +91,8 @@ typedef struct gexs_lines {
     const double*  gamma;  /* Lorentz half-width at T_ref, 1 atm [cm^-1]   */
     const double*  n;      /* temperature exponent of gamma                */
     int64_t        count;
+    int32_t        format; /* GEXS_LINES_FP64 or GEXS_LINES_COMPACT        */
+    int32_t        reserved;
 } gexs_lines;
 
 /* ------------------------------------------------------------------ jobs

@@ -230,3 +230,22 @@ def test_gauss_hermite_fp32_across_pressures(gpu_ctx, small_lines, nodes, P):
     job = _make(small_lines, capi.FP32, capi.VOIGT_QUAD, nodes, capi.CONV_PHYSICAL, T=2500.0,
                 P=P, nu0=1000.0, dnu=0.01, G=150000, cutoff=25.0)
     _check(gpu_ctx, job, small_lines)
+
+
+@pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
+@pytest.mark.parametrize("name,profile,nodes", [("voigt", capi.VOIGT, 16),
+                                                ("doppler", capi.DOPPLER, 16),
+                                                ("gh16", capi.VOIGT_QUAD, 16)])
+def test_compact_line_list(gpu_ctx, small_lines, name, profile, nodes, prec):
+    """GEXS_LINES_COMPACT (FP64 nu, float E'', g'A, gamma, n): the kernels
+    compute on the widened floats, so the results match the oracle given
+    those same values (g' = 1) with the usual tolerances; derive-on-load
+    rejects the format."""
+    cl = LineList(small_lines["nu"], small_lines["elow"], small_lines["aif"], small_lines["gns"],
+                  small_lines["gamma"], small_lines["n"], compact=True)
+    assert cl.elow.dtype == torch.float32 and cl.gns is None
+    job = _make(small_lines, prec, profile, nodes, capi.CONV_PHYSICAL, lines_dev=cl)
+    _check(gpu_ctx, job, cl.widened())
+    bad = _make(small_lines, prec, profile, nodes, capi.CONV_PHYSICAL, lines_dev=cl)
+    with pytest.raises(capi.GexsError):
+        gpu_ctx.run([bad], cfg=(4, 8, 0, capi.LAUNCH_DERIVE_ON_LOAD))
