@@ -565,13 +565,18 @@ template <int B>
 __device__ __forceinline__ void voigt_full2(const RecV& p, const RecV& q, float2 lw2,
                                             float2 (&part)[B / 2])
 {
-    const float2 step = make_float2(64.f, 64.f);
+    const float2 s64 = make_float2(64.f, 64.f);
     const float2 pdx = p.dx, pmf = p.mf, pc = p.c, py2 = p.y2, pa = p.a;
     const float2 qdx = q.dx, qmf = q.mf, qc = q.c, qy2 = q.y2, qa = q.a;
-    float2 np = __fadd2_rn(p.nb, lw2), nq = __fadd2_rn(q.nb, lw2);
+    /* x of the lane's first pair from the exact integer n, one rounding;
+     * each later pair is 64 bins further: x += 64 dx (64 dx exact), one
+     * rounding more per pair */
+    float2 xp = __ffma2_rn(__fadd2_rn(p.nb, lw2), pdx, pmf);
+    float2 xq = __ffma2_rn(__fadd2_rn(q.nb, lw2), qdx, qmf);
+    const float2 sp = __fmul2_rn(pdx, s64), sq = __fmul2_rn(qdx, s64);
 #pragma unroll
     for (int j = 0; j < B / 2; ++j) {
-        const float2 xp = __ffma2_rn(np, pdx, pmf), xq = __ffma2_rn(nq, qdx, qmf);
+        if (j) { xp = __fadd2_rn(xp, sp); xq = __fadd2_rn(xq, sq); }
         const float2 mp = __ffma2_rn(xp, xp, pc), mq = __ffma2_rn(xq, xq, qc);
         const float2 dp = __ffma2_rn(mp, mp, py2), dq = __ffma2_rn(mq, mq, qy2);
         float2 rp, rq;
@@ -579,7 +584,25 @@ __device__ __forceinline__ void voigt_full2(const RecV& p, const RecV& q, float2
         rq.x = rcp_approx(dq.x); rq.y = rcp_approx(dq.y);
         const float2 tp = __ffma2_rn(mp, rp, rp), tq = __ffma2_rn(mq, rq, rq);
         part[j] = __ffma2_rn(tq, qa, __ffma2_rn(tp, pa, part[j]));
-        np = __fadd2_rn(np, step); nq = __fadd2_rn(nq, step);
+    }
+}
+
+/* one full-tier record, as voigt_full2 */
+template <int B>
+__device__ __forceinline__ void voigt_full1(const RecV& p, float2 lw2, float2 (&part)[B / 2])
+{
+    const float2 s64 = make_float2(64.f, 64.f);
+    const float2 pdx = p.dx, pmf = p.mf, pc = p.c, py2 = p.y2, pa = p.a;
+    float2 xp = __ffma2_rn(__fadd2_rn(p.nb, lw2), pdx, pmf);
+    const float2 sp = __fmul2_rn(pdx, s64);
+#pragma unroll
+    for (int j = 0; j < B / 2; ++j) {
+        if (j) xp = __fadd2_rn(xp, sp);
+        const float2 mp = __ffma2_rn(xp, xp, pc);
+        const float2 dp = __ffma2_rn(mp, mp, py2);
+        float2 rp;
+        rp.x = rcp_approx(dp.x); rp.y = rcp_approx(dp.y);
+        part[j] = __ffma2_rn(__ffma2_rn(mp, rp, rp), pa, part[j]);
     }
 }
 
@@ -655,6 +678,17 @@ __device__ __forceinline__ void voigt_full4(const RecV* __restrict__ r, float2 l
     }
     voigt_full2<B>(q[0], q[1], lw2, part);
     voigt_full2<B>(q[2], q[3], lw2, part);
+}
+
+/* records that are full-tier for every consumer warp: no tier tests */
+template <int B>
+__device__ __forceinline__ void lines_voigt_allfull(const RecV* __restrict__ rec, int nrec,
+                                                    float2 lw2, float2 (&part)[B / 2])
+{
+    int i = 0;
+    for (; i + 3 < nrec; i += 4) voigt_full4<B>(rec + i, lw2, part);
+    if (i + 1 < nrec) { voigt_full2<B>(rec[i], rec[i + 1], lw2, part); i += 2; }
+    if (i < nrec) voigt_full1<B>(rec[i], lw2, part);
 }
 
 template <int B>
@@ -1020,6 +1054,13 @@ constexpr int WS_STAGES = 4;
 constexpr int WS_R = 128;
 constexpr int WS_SPIN = 1 << 21;          /* default try_wait attempts before giving up */
 
+/* A stage's records are written in PROD regions of WS_R / PROD slots, one
+ * per producer warp; in region w the nf[w] records that are full-tier for
+ * every consumer warp come first (slots 0.., in line order) and the nn[w]
+ * others last (slots from the end downwards, in line order): consumers take
+ * the first block without any tier test.  The order in which a bin sums its
+ * lines is therefore a fixed function of the tile's lines. */
+constexpr int WS_MAX_PROD = 4;
 struct StageHdr {
     long long j0;          /* absolute first bin of the tile                */
     int jl;                /* job index                                     */
@@ -1028,6 +1069,8 @@ struct StageHdr {
     int flags;             /* 1 first stage of the tile, 2 last, 4 end,
                               8 the item is one slice of a split tile       */
     int item, tile;        /* work item and its tile                        */
+    int nf[WS_MAX_PROD];   /* all-full records of each producer region      */
+    int nn[WS_MAX_PROD];   /* other records of each producer region         */
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
@@ -1085,7 +1128,11 @@ voigt_ws_kernel(const KArgs args)
     typedef WsSmem<B, CONS, PROD, PREP> L;
     constexpr int NP = L::NP, W = L::W;
     constexpr int SUB = WS_R / NP;               /* lines per producer thread per stage */
+    constexpr int WR = WS_R / PROD;              /* records per producer region */
+    /* tier code 1 (full) for every consumer warp */
+    constexpr int kAllFull = 0x55555555 & ((1 << (2 * CONS)) - 1);
     static_assert(WS_R % NP == 0, "stage size must be a multiple of the producer threads");
+    static_assert(PROD <= WS_MAX_PROD && CONS <= 8, "launch shape");
     extern __shared__ __align__(16) unsigned char smem[];
     RecV* s_rec = reinterpret_cast<RecV*>(smem + L::off_rec);
     StageHdr* s_hdr = reinterpret_cast<StageHdr*>(smem + L::off_hdr);
@@ -1212,14 +1259,18 @@ voigt_ws_kernel(const KArgs args)
                 if (!mbar_wait(s_empty + st, ph, args.spin)) { fail(); return; }
                 const int64_t pbase = lo + (int64_t)c * WS_R;
                 const int nrec = (int)max((int64_t)0, min((int64_t)WS_R, hi - pbase));
-                RecV* rec = s_rec + st * WS_R;
+                /* this producer warp's region of the stage */
+                RecV* reg = s_rec + st * WS_R + pw * WR;
+                int nf = 0, nn = 0;
 #pragma unroll
                 for (int sub = 0; sub < SUB; ++sub) {
                     const int u = c * SUB + sub;
                     const int o = (u & 1) * NP + ptid;
                     cp_async_wait<1>();
                     const int r = sub * NP + ptid;
-                    if (r < nrec) {
+                    const bool valid = r < nrec;
+                    RecV rr;
+                    if (valid) {
                         LineQ lq;
                         if constexpr (PREP) {
                             const double nu = s_f[o];
@@ -1232,19 +1283,25 @@ voigt_ws_kernel(const KArgs args)
                             lq = line_quantities<true>(J, Lr);
                         }
                         Derived<PK_VOIGT> d = derive_line_body<PK_VOIGT>(T, lq, 10.5);
-                        RecV rr;
                         make_rec<PK_VOIGT, B, CONS>(rr, d, J, T);
-                        rec[r] = rr;
                     }
+                    const bool full = valid && rr.tiers == kAllFull;
+                    const unsigned bf = __ballot_sync(0xffffffffu, full);
+                    const unsigned bn = __ballot_sync(0xffffffffu, valid && !full);
+                    const unsigned below = (1u << lane) - 1u;
+                    if (full) reg[nf + __popc(bf & below)] = rr;
+                    else if (valid) reg[WR - 1 - (nn + __popc(bn & below))] = rr;
+                    nf += __popc(bf);
+                    nn += __popc(bn);
                     issue(u + 2);
                 }
+                if (lane == 0) { s_hdr[st].nf[pw] = nf; s_hdr[st].nn[pw] = nn; }
                 if (ptid == 0) {
-                    StageHdr h;
+                    StageHdr& h = s_hdr[st];
                     h.j0 = T.j0; h.jl = jl; h.jn = T.jn; h.nrec = nrec;
                     h.flags = (c == 0 ? 1 : 0) | (c == nchunk - 1 ? 2 : 0) | (ns > 1 ? 8 : 0);
                     h.item = item;
                     h.tile = ti;
-                    s_hdr[st] = h;
                 }
                 mbar_arrive(s_full + st);
                 if (++st == WS_STAGES) { st = 0; ph ^= 1; }
@@ -1283,7 +1340,16 @@ voigt_ws_kernel(const KArgs args)
             }
         }
         const RecV* rec = s_rec + st * WS_R;
-        lines_voigt_f32<B>(rec, h.nrec, warp, lane, part);
+        {
+            const float lw = (float)(warp * 32 * B + lane);
+            const float2 lw2 = make_float2(lw, lw);
+#pragma unroll
+            for (int w = 0; w < PROD; ++w) {
+                const RecV* reg = rec + w * WR;
+                lines_voigt_allfull<B>(reg, h.nf[w], lw2, part);
+                lines_voigt_f32<B>(reg + WR - h.nn[w], h.nn[w], warp, lane, part);
+            }
+        }
 #pragma unroll
         for (int k = 0; k < B; ++k) {
             const int t = warp * 32 * B + lane + 32 * k;
