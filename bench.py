@@ -25,6 +25,7 @@ also   = plain FP64 per-(T,P) GPU path on the same workload, the 64-pair
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -32,6 +33,16 @@ import sys
 import time
 
 import numpy as np
+
+# a crash in native code prints the Python stack of every thread to stderr
+faulthandler.enable()
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """progress on stderr (stdout carries only the JSON line)"""
+    sys.stderr.write("[bench %7.1f s] %s\n" % (time.perf_counter() - _T0, msg))
+    sys.stderr.flush()
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -578,6 +589,7 @@ def serve_bench(torch, dev, local_rank, args):
             raise RuntimeError(errors[0])
         return wall, np.array(lat), np.array(dlat), infos
 
+    log("serving: %d requests, serial pass" % len(reqs))
     # warm-up (module loads, pools), then the set one request at a time
     for _, rq in reqs[:3]:
         srv.wait(srv.submit(rq), rq.grid_points)
@@ -596,6 +608,7 @@ def serve_bench(torch, dev, local_rank, args):
     rates = []
     for k, load in enumerate(args.serve_loads):
         rate = load / service
+        log("serving: offered load %.2f" % load)
         wall, lat, dlat, infos = run(rate, 4100 + k)
         rates.append({"offered_load": load, "offered_req_per_s": rate, "requests": len(reqs),
                       "p50_ms": float(np.percentile(lat, 50)),
@@ -778,6 +791,7 @@ def our_arm(args):
     torch.cuda.set_device(local_rank)
     from gexs_b200 import Context, Job, LineList, synth, _capi as capi
 
+    log("generating the %d-line list" % args.lines)
     st = synth.make_states(200000, 80, 1002)
     L = synth.make_lines_torch(st, args.lines, NU0, NU1, 2002, broadening_seed=3002, device=dev)
     lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev)
@@ -806,6 +820,7 @@ def our_arm(args):
         (tuple(int(v) for v in args.cfg.split(",")), 0.0)
     stream = torch.cuda.current_stream(dev)
 
+    log("warm-up")
     for _ in range(args.warmup):
         ctx.run([job], cfg=cfg, stream=stream)
     ctx.check(stream)
@@ -832,6 +847,7 @@ def our_arm(args):
     value = evals_all * args.steps / (ms_max * 1e-3)
     launch_ms = ms / args.steps
 
+    log("timed region done; plain FP64 path")
     # plain FP64 per-(T,P) path on the same workload
     out64 = torch.zeros(G, dtype=torch.float64, device=dev)
     j64 = Job(lines, out64, convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=T_K,
@@ -848,10 +864,12 @@ def our_arm(args):
     integral = float(out64.sum()) * DNU
     vs_oracle = None
     if rank == 0 and not args.no_cpu and (start_idx, n_points) == (0, G):
+        log("oracle sub-band")
         vs_oracle = oracle_subband(torch, L, q, {"fp32": (out, capi.FP32),
                                                  "fp64": (out64, capi.FP64)})
     del out64, j64
 
+    log("e2e through the manager")
     # e2e through the manager C ABI, host buffers
     e2e_s, h2d, d2h, e2e_res = e2e_manager(torch, dev, L, q, args.steps, min(args.warmup, 1),
                                            local_rank)
@@ -864,6 +882,7 @@ def our_arm(args):
 
     result = None
     if rank == 0:
+        log("probes and FLOP accounting")
         peak = 0.0
         import ctypes as C
         from gexs_b200._capi import lib
@@ -944,17 +963,22 @@ def our_arm(args):
             "clocks": clocks,
         }
     if not args.no_cpu and rank == 0 and ws == 1:
+        log("reference GPU kernel")
         result["reference_gpu_kernel"] = gpu_reference_sample(torch, ctx, L, q, dev)
     if not args.no_batch and rank == 0:
+        log("64-pair batch on the 1e6-line list")
         result["batch64"] = batch64(ctx, torch, dev)
+        log("64 pairs of the 1e8-line list")
         result["batch_64_pairs_1e8_lines"] = batch_north_star(
             ctx, torch, dev, lines, st, result["roofline"]["flop_per_eval"],
             result["roofline"].get("fp64_peak_tflops"), cfg)
     if not args.no_serve and rank == 0:
+        log("serving loop")
         del lines, job, out, L
         torch.cuda.empty_cache()
         result["serve"] = serve_bench(torch, dev, local_rank, args)
     if not args.no_cpu and rank == 0 and ws == 1:
+        log("CPU baseline")
         v, cores, sample, kind = cpu_reference_sample(target_s=args.cpu_seconds)
         result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                                   "sample": sample}
