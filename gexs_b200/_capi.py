@@ -49,8 +49,7 @@ class GexsJob(C.Structure):
 
 class GexsLaunchCfg(C.Structure):
     _fields_ = [("bins_per_lane", C.c_int32), ("warps", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("flags", C.c_int32), ("wait_spins", C.c_int32),
-                ("pairs", C.c_int32), ("lines_per_stage", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("flags", C.c_int32), ("wait_spins", C.c_int32)]
 
 LAUNCH_DERIVE_ON_LOAD = 1
 

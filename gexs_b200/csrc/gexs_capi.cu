@@ -106,9 +106,7 @@ static bool cfg_ok(const gexs_launch_cfg& c, int prec)
     /* 16 bins per lane only for the FP32 form */
     return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8 ||
             (c.bins_per_lane == 16 && prec == GEXS_FP32)) &&
-           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0 &&
-           (c.pairs == 0 || c.pairs == 1 || c.pairs == 2 || c.pairs == 4) &&
-           (c.lines_per_stage == 0 || c.lines_per_stage == 64 || c.lines_per_stage == 128);
+           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0;
 }
 
 static gexs_launch_cfg ctx_cfg(gexs_ctx* ctx, int pk, int prec)
@@ -124,46 +122,7 @@ struct Group {
     std::vector<gexs_job> jobs;
     std::vector<int> prefix;
     int nitems = 0;
-    /* FP32 Voigt with pairs > 1: packs of jobs that share the grid, the
-     * cutoff, the window rule and the line list; the region-I kernel's
-     * items are the packs' tiles */
-    int pp = 1;
-    std::vector<int> pk_prefix, pk_jobs;
 };
-
-/* jobs whose tiles find the same lines in the same order */
-static bool same_tiles(const gexs_job& a, const gexs_job& b)
-{
-    return a.lines.nu == b.lines.nu && a.lines.count == b.lines.count &&
-           a.lines.format == b.lines.format && a.lines.elow == b.lines.elow &&
-           a.lines.aif == b.lines.aif && a.lines.gns == b.lines.gns &&
-           a.lines.gamma == b.lines.gamma && a.lines.n == b.lines.n &&
-           a.nu_start == b.nu_start && a.dnu == b.dnu && a.grid_points == b.grid_points &&
-           a.start_idx == b.start_idx && a.n_points == b.n_points && a.cutoff == b.cutoff &&
-           a.window_rule == b.window_rule;
-}
-
-/* greedy packs of up to pp jobs in job order */
-static void make_packs(Group& g, int pp, int W)
-{
-    g.pp = pp;
-    g.pk_prefix.assign(1, 0);
-    g.pk_jobs.clear();
-    std::vector<int> fill;       /* jobs in each pack */
-    for (int i = 0; i < (int)g.jobs.size(); ++i) {
-        int k = -1;
-        for (int q = 0; q < (int)fill.size(); ++q)
-            if (fill[q] < pp && same_tiles(g.jobs[g.pk_jobs[(size_t)q * pp]], g.jobs[i])) { k = q; break; }
-        if (k < 0) {
-            k = (int)fill.size();
-            fill.push_back(0);
-            g.pk_jobs.resize(g.pk_jobs.size() + pp, -1);
-            const int64_t tiles = (g.jobs[i].n_points + W - 1) / W;
-            g.pk_prefix.push_back(g.pk_prefix.back() + (int)tiles);
-        }
-        g.pk_jobs[(size_t)k * pp + fill[k]++] = i;
-    }
-}
 
 static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg_in,
                         gexs_ctx* ctx, std::vector<Group>& groups,
@@ -194,9 +153,6 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
         g.nitems += (int)tiles;
         g.prefix.push_back(g.nitems);
     }
-    for (size_t k = 0; k < groups.size(); ++k)
-        if (groups[k].pk == PK_VOIGT && groups[k].prec == GEXS_FP32 && cfgs[k].pairs > 1)
-            make_packs(groups[k], cfgs[k].pairs, tile_bins(cfgs[k]));
     return GEXS_OK;
 }
 
@@ -205,7 +161,6 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
  * prep arrays only when the group derives per job (the default). */
 struct Layout {
     size_t op, oc, opp, oprep, bytes;
-    size_t opk_prefix = 0, opk_jobs = 0;   /* pack tables (packs only) */
     std::vector<size_t> job_prep;   /* byte offset of each job's prep arrays */
     /* line-slice tables (FP32 Voigt groups): offsets, item bound, lines per slice */
     bool sliced = false;
@@ -230,12 +185,6 @@ static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg
     a = up(a + g.prefix.size() * sizeof(int));
     L.oc = a;
     a += 256;
-    if (!g.pk_jobs.empty()) {
-        L.opk_prefix = a;
-        a = up(a + g.pk_prefix.size() * sizeof(int));
-        L.opk_jobs = a;
-        a = up(a + g.pk_jobs.size() * sizeof(int));
-    }
     L.opp = a;
     a = up(a + g.jobs.size() * sizeof(double*));
     L.oprep = a;
@@ -246,23 +195,12 @@ static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg
     if (slices_apply(g.pk, g.prec) && g.nitems > 0) {
         const int W = tile_bins(cfg);
         const size_t nt = (size_t)g.nitems;
-        /* tickets per (tile, pair) for packs: at most pack tiles x pp */
-        const size_t ntk = g.pk_jobs.empty() ? nt
-                                             : std::max(nt, (size_t)g.pk_prefix.back() * (size_t)g.pp);
         L.sliced = true;
-        if (g.pk_jobs.empty()) {
-            L.lines_per_slice = slice_lines(g.jobs.data(), (int)g.jobs.size(), W, &L.max_rows);
-        } else {
-            /* a pack's split tiles keep pp rows per slice, filled or not */
-            std::vector<gexs_job> rep;
-            for (size_t k = 0; k + 1 < g.pk_prefix.size(); ++k)
-                for (int q = 0; q < g.pp; ++q) rep.push_back(g.jobs[g.pk_jobs[k * g.pp]]);
-            L.lines_per_slice = slice_lines(rep.data(), (int)rep.size(), W, &L.max_rows);
-        }
+        L.lines_per_slice = slice_lines(g.jobs.data(), (int)g.jobs.size(), W, &L.max_rows);
         L.os_prefix = up(a); a = L.os_prefix + (nt + 1) * sizeof(int);
         L.os_counts = up(a); a = L.os_counts + nt * sizeof(int);
         L.os_rowbase = up(a); a = L.os_rowbase + nt * sizeof(int);
-        L.os_ticket = up(a); a = L.os_ticket + ntk * sizeof(int);
+        L.os_ticket = up(a); a = L.os_ticket + nt * sizeof(int);
         L.os_lohi = up(a);   a = L.os_lohi + 2 * nt * sizeof(long long);
         L.os_nitems = up(a); a = L.os_nitems + 256;
         L.os_rows = up(a);   a = L.os_rows + (size_t)L.max_rows * W * sizeof(double);
@@ -288,10 +226,6 @@ static std::vector<unsigned char> group_image(const Group& g, const Layout& L, u
     std::vector<unsigned char> h(L.oprep, 0);
     std::memcpy(h.data(), g.jobs.data(), g.jobs.size() * sizeof(gexs_job));
     std::memcpy(h.data() + L.op, g.prefix.data(), g.prefix.size() * sizeof(int));
-    if (!g.pk_jobs.empty()) {
-        std::memcpy(h.data() + L.opk_prefix, g.pk_prefix.data(), g.pk_prefix.size() * sizeof(int));
-        std::memcpy(h.data() + L.opk_jobs, g.pk_jobs.data(), g.pk_jobs.size() * sizeof(int));
-    }
     double** pp = reinterpret_cast<double**>(h.data() + L.opp);
     for (size_t i = 0; i < g.jobs.size(); ++i)
         pp[i] = prep ? reinterpret_cast<double*>(dev + L.job_prep[i]) : nullptr;
@@ -346,16 +280,10 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
         csl.max_rows = L.cmax_rows;
         csl.lines_per_slice = L.clines_per_slice;
     }
-    PackTables pk;
-    pk.prefix = g.pk_jobs.empty() ? nullptr : (const int*)(d + L.opk_prefix);
-    pk.jobs = g.pk_jobs.empty() ? nullptr : (const int*)(d + L.opk_jobs);
-    pk.npacks = (int)g.pk_prefix.size() - 1;
-    pk.pp = g.pp;
-    pk.nitems = g.pk_prefix.empty() ? 0 : g.pk_prefix.back();
     return launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + L.op),
                         (int)g.jobs.size(), g.nitems, (int*)(d + L.oc), d_err,
                         prep ? pp : nullptr, cfg, nsm, s, L.sliced ? &sl : nullptr,
-                        L.csliced ? &csl : nullptr, g.pk_jobs.empty() ? nullptr : &pk);
+                        L.csliced ? &csl : nullptr);
 }
 
 extern "C" {
@@ -713,45 +641,25 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     float best_ms = 1e30f; gexs_launch_cfg bc = default_cfg(pk, prec);
     int st = GEXS_OK;
-    /* time one launch shape on the jobs (best of two after a warm-up) */
-    auto trial = [&](const gexs_launch_cfg& c) {
-        gexs_batch* b = nullptr;
-        st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);
-        if (st) return;
-        float ms = 1e30f;
-        for (int rep = 0; rep < 3 && !st; ++rep) {
-            cudaEventRecord(e0, s);
-            st = gexs_batch_launch(b, s);
-            cudaEventRecord(e1, s);
-            if (cudaEventSynchronize(e1) != cudaSuccess) st = set_error(GEXS_ERR_CUDA, "autotune run");
-            float t = 0.f; cudaEventElapsedTime(&t, e0, e1);
-            if (rep > 0) ms = std::min(ms, t);        /* first run warms up */
-        }
-        gexs_batch_destroy(b);
-        if (!st && ms < best_ms) { best_ms = ms; bc = c; }
-    };
-    /* tile width: bins per lane x warps */
     for (int bi = 0; bi < nbins && !st; ++bi)
         for (int wi = 0; wi < 2 && !st; ++wi) {
             gexs_launch_cfg c{}; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
-            trial(c);
+            c.ctas_per_sm = 0; c.flags = 0;
+            gexs_batch* b = nullptr;
+            st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);
+            if (st) break;
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && !st; ++rep) {
+                cudaEventRecord(e0, s);
+                st = gexs_batch_launch(b, s);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) st = set_error(GEXS_ERR_CUDA, "autotune run");
+                float t = 0.f; cudaEventElapsedTime(&t, e0, e1);
+                if (rep > 0) ms = std::min(ms, t);        /* first run warms up */
+            }
+            gexs_batch_destroy(b);
+            if (!st && ms < best_ms) { best_ms = ms; bc = c; }
         }
-    /* FP32 Voigt: lines per stage, then pairs per CTA when jobs share a grid */
-    if (!st && pk == PK_VOIGT && prec == GEXS_FP32) {
-        gexs_launch_cfg c = bc;
-        c.lines_per_stage = 64;
-        trial(c);
-        bool shared = false;
-        for (int i = 1; i < njobs && !shared; ++i)
-            for (int k = 0; k < i && !shared; ++k) shared = same_tiles(tj[k], tj[i]);
-        const gexs_launch_cfg base = bc;
-        for (int pp : {2, 4}) {
-            if (!shared || st) break;
-            gexs_launch_cfg c2 = base;
-            c2.pairs = pp;
-            trial(c2);
-        }
-    }
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     cudaStreamDestroy(s);
     if (st) return st;

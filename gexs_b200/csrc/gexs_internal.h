@@ -7,9 +7,6 @@
 
 namespace gexs {
 
-/* profile classes of the kernel templates (profile_class) */
-enum { PK_VOIGT = 0, PK_ERF = 1, PK_GH16 = 2, PK_GH32 = 3 };
-
 /* kernel launchers (gexs_kernels.cu; tile kernels in gexs_tiles.cuh) */
 int profile_class(const gexs_job& j);
 int tile_bins(const gexs_launch_cfg& c);
@@ -40,17 +37,11 @@ struct SliceTables {
  * d_counter: a 256-byte block of work counters; the caller zeroes the
  * first int, the FP32 Voigt core kernel's counter (int 32) is zeroed here
  * (by zero_ints). */
-/* packs of pairs of the FP32 Voigt region-I kernel: device tables */
-struct PackTables {
-    const int* prefix;   /* npacks + 1: first tile of each pack            */
-    const int* jobs;     /* npacks * pp: job of each pair (-1: none)       */
-    int npacks, pp, nitems;
-};
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
                          cudaStream_t st, const SliceTables* sl = nullptr,
-                         const SliceTables* csl = nullptr, const PackTables* packs = nullptr);
+                         const SliceTables* csl = nullptr);
 /* which groups are sliced (all); lines_per_slice for a group (grows only
  * when the partial rows of its split tiles could pass 1 GiB) and the bound
  * on those rows */

@@ -128,24 +128,13 @@ int profile_class(const gexs_job& j)
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st, const SliceTables* sl, const SliceTables* csl,
-                         const PackTables* packs)
+                         cudaStream_t st, const SliceTables* sl, const SliceTables* csl)
 {
     KArgs a;
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
     a.counter = d_counter; a.err = d_err; a.prep = d_prep;
     a.tile_w = tile_bins(cfg);
     a.spin = cfg.wait_spins > 0 ? cfg.wait_spins : WS_SPIN;
-    a.pk_jobs = nullptr;
-    a.pp = 1;
-    a.pk_prefix = nullptr;
-    a.npacks = 0;
-    a.pk_nitems = 0;
-    if (packs && packs->pp > 1 && pk == PK_VOIGT && prec == GEXS_FP32) {
-        a.pk_jobs = packs->jobs; a.pp = packs->pp; a.pk_prefix = packs->prefix;
-        a.npacks = packs->npacks; a.pk_nitems = packs->nitems;
-    }
-    a.lps = cfg.lines_per_stage == 64 ? 64 : 128;
     std::memset(&a.sl, 0, sizeof(a.sl));
     std::memset(&a.csl, 0, sizeof(a.csl));
     if (sl && slices_apply(pk, prec)) a.sl = *sl;
@@ -180,10 +169,9 @@ __global__ void slice_plan_kernel(const KArgs a)
     const int lane = threadIdx.x & 31;
     const int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ti >= a.nitems) return;
-    /* the tile's job (the first pair's, when the items are pack tiles) */
     int jl = 0, jh = a.njobs;
     while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
-    const gexs_job& J = a.jobs[a.pk_jobs ? __ldg(a.pk_jobs + jl * a.pp) : jl];
+    const gexs_job& J = a.jobs[jl];
     const int64_t j0 = J.start_idx + (int64_t)(ti - __ldg(a.prefix + jl)) * a.tile_w;
     const int jn = (int)min((int64_t)a.tile_w, J.start_idx + J.n_points - j0);
     const double f0 = grid_f(J.nu_start, J.dnu, j0);
@@ -197,10 +185,8 @@ __global__ void slice_plan_kernel(const KArgs a)
         a.sl.lohi[2 * ti] = lo;
         a.sl.lohi[2 * ti + 1] = hi;
         a.sl.counts[ti] = n > per ? (int)((n + per - 1) / per) : 1;
+        a.sl.ticket[ti] = 0;
     }
-    /* one ticket per (tile, pair) */
-    const int pp = a.pk_jobs ? a.pp : 1;
-    if (lane < pp) a.sl.ticket[ti * pp + lane] = 0;
 }
 
 /* the same for the FP32 Voigt core kernel: its line range per tile is the
@@ -264,9 +250,7 @@ __global__ void __launch_bounds__(1024) slice_scan_kernel(const KArgs a)
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        /* split tiles of packs keep one partial row per pair */
-        const long long rows = rcarry * (long long)(a.pk_jobs ? a.pp : 1);
-        if (rows > a.sl.max_rows || carry > INT32_MAX) {
+        if (rcarry > a.sl.max_rows || carry > INT32_MAX) {
             /* cannot happen with the host's bound; run no item rather than
              * write past the partial rows */
             atomicOr(a.err, GEXS_KERR_SLICES);

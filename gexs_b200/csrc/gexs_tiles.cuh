@@ -38,6 +38,8 @@
 
 namespace gexs {
 
+/* profile classes of the kernel template */
+enum { PK_VOIGT = 0, PK_ERF = 1, PK_GH16 = 2, PK_GH32 = 3 };
 
 /* --------------------------------------------------------------- records
  * One derived record per (line, tile), written by the thread that derived
@@ -259,17 +261,16 @@ __device__ __forceinline__ LineQ line_quantities(const gexs_job& J, const RawLin
 /* tile-dependent part: centre in bins, window and Humlicek region limits
  * (inlined into the warp-specialised producers; derive_line below is the
  * out-of-line form for kernels that interleave it with their FP32 loops) */
-/* the line's quantities with its centre tc (tile-relative bins) and its
- * window [a, b) in the tile already known */
 template <int PK>
-__device__ __forceinline__ Derived<PK> derive_line_win(const Tile& T, const LineQ& q, double zthr,
-                                                       double tc, int a, int b)
+__device__ __forceinline__ Derived<PK> derive_line_body(const Tile& T, const LineQ& q, double zthr)
 {
     const gexs_job& J = *T.J;
     Derived<PK> d;
     const double nu = q.nu;
     d.nu = nu; d.S = q.S; d.invw = q.invw; d.y = q.y;
-    d.tc = tc;
+    d.tc = dmul(dsub(nu, T.f0), T.inv_dnu);
+    int a, b;
+    tile_window(T, nu, d.tc, &a, &b);
     d.win = pack2(a, b);
     d.c1 = d.c2 = d.c3 = 0;
     if (a >= b || d.S == 0.0) { d.win = 0; return d; }
@@ -301,15 +302,6 @@ __device__ __forceinline__ Derived<PK> derive_line_win(const Tile& T, const Line
 }
 
 template <int PK>
-__device__ __forceinline__ Derived<PK> derive_line_body(const Tile& T, const LineQ& q, double zthr)
-{
-    const double tc = dmul(dsub(q.nu, T.f0), T.inv_dnu);
-    int a, b;
-    tile_window(T, q.nu, tc, &a, &b);
-    return derive_line_win<PK>(T, q, zthr, tc, a, b);
-}
-
-template <int PK>
 __device__ __noinline__ Derived<PK> derive_line(const Tile& T, const LineQ& q, double zthr)
 {
     return derive_line_body<PK>(T, q, zthr);
@@ -328,16 +320,6 @@ struct KArgs {
     SliceTables     sl;        /* line slices (sl.prefix NULL: none)     */
     SliceTables     csl;       /* FP32 Voigt core kernel's slices        */
     int             spin;      /* try_wait attempts of every bounded wait */
-    /* FP32 Voigt region-I kernel only: packs of pairs that share a grid and
-     * a line list.  When pk_jobs is set, prefix / njobs / nitems describe
-     * the packs (tiles of each pack) and pk_jobs[k * pp + p] is the job of
-     * pair p of pack k (-1: none); otherwise every job is a pack of one. */
-    const int*      pk_jobs;
-    int             pp;        /* pairs per pack                          */
-    int             lps;       /* lines per stage: 64 or 128              */
-    const int*      pk_prefix; /* npacks + 1: first tile of each pack      */
-    int             npacks;
-    int             pk_nitems; /* tiles of all packs                       */
 };
 
 /* slice_plan_kernel + slice_scan_kernel (gexs_kernels.cu): every tile's
@@ -583,18 +565,13 @@ template <int B>
 __device__ __forceinline__ void voigt_full2(const RecV& p, const RecV& q, float2 lw2,
                                             float2 (&part)[B / 2])
 {
-    const float2 s64 = make_float2(64.f, 64.f);
+    const float2 step = make_float2(64.f, 64.f);
     const float2 pdx = p.dx, pmf = p.mf, pc = p.c, py2 = p.y2, pa = p.a;
     const float2 qdx = q.dx, qmf = q.mf, qc = q.c, qy2 = q.y2, qa = q.a;
-    /* x of the lane's first pair from the exact integer n, one rounding;
-     * each later pair is 64 bins further: x += 64 dx (64 dx exact), one
-     * rounding more per pair */
-    float2 xp = __ffma2_rn(__fadd2_rn(p.nb, lw2), pdx, pmf);
-    float2 xq = __ffma2_rn(__fadd2_rn(q.nb, lw2), qdx, qmf);
-    const float2 sp = __fmul2_rn(pdx, s64), sq = __fmul2_rn(qdx, s64);
+    float2 np = __fadd2_rn(p.nb, lw2), nq = __fadd2_rn(q.nb, lw2);
 #pragma unroll
     for (int j = 0; j < B / 2; ++j) {
-        if (j) { xp = __fadd2_rn(xp, sp); xq = __fadd2_rn(xq, sq); }
+        const float2 xp = __ffma2_rn(np, pdx, pmf), xq = __ffma2_rn(nq, qdx, qmf);
         const float2 mp = __ffma2_rn(xp, xp, pc), mq = __ffma2_rn(xq, xq, qc);
         const float2 dp = __ffma2_rn(mp, mp, py2), dq = __ffma2_rn(mq, mq, qy2);
         float2 rp, rq;
@@ -602,25 +579,7 @@ __device__ __forceinline__ void voigt_full2(const RecV& p, const RecV& q, float2
         rq.x = rcp_approx(dq.x); rq.y = rcp_approx(dq.y);
         const float2 tp = __ffma2_rn(mp, rp, rp), tq = __ffma2_rn(mq, rq, rq);
         part[j] = __ffma2_rn(tq, qa, __ffma2_rn(tp, pa, part[j]));
-    }
-}
-
-/* one full-tier record, as voigt_full2 */
-template <int B>
-__device__ __forceinline__ void voigt_full1(const RecV& p, float2 lw2, float2 (&part)[B / 2])
-{
-    const float2 s64 = make_float2(64.f, 64.f);
-    const float2 pdx = p.dx, pmf = p.mf, pc = p.c, py2 = p.y2, pa = p.a;
-    float2 xp = __ffma2_rn(__fadd2_rn(p.nb, lw2), pdx, pmf);
-    const float2 sp = __fmul2_rn(pdx, s64);
-#pragma unroll
-    for (int j = 0; j < B / 2; ++j) {
-        if (j) xp = __fadd2_rn(xp, sp);
-        const float2 mp = __ffma2_rn(xp, xp, pc);
-        const float2 dp = __ffma2_rn(mp, mp, py2);
-        float2 rp;
-        rp.x = rcp_approx(dp.x); rp.y = rcp_approx(dp.y);
-        part[j] = __ffma2_rn(__ffma2_rn(mp, rp, rp), pa, part[j]);
+        np = __fadd2_rn(np, step); nq = __fadd2_rn(nq, step);
     }
 }
 
@@ -696,17 +655,6 @@ __device__ __forceinline__ void voigt_full4(const RecV* __restrict__ r, float2 l
     }
     voigt_full2<B>(q[0], q[1], lw2, part);
     voigt_full2<B>(q[2], q[3], lw2, part);
-}
-
-/* records that are full-tier for every consumer warp: no tier tests */
-template <int B>
-__device__ __forceinline__ void lines_voigt_allfull(const RecV* __restrict__ rec, int nrec,
-                                                    float2 lw2, float2 (&part)[B / 2])
-{
-    int i = 0;
-    for (; i + 3 < nrec; i += 4) voigt_full4<B>(rec + i, lw2, part);
-    if (i + 1 < nrec) { voigt_full2<B>(rec[i], rec[i + 1], lw2, part); i += 2; }
-    if (i < nrec) voigt_full1<B>(rec[i], lw2, part);
 }
 
 template <int B>
@@ -1072,13 +1020,6 @@ constexpr int WS_STAGES = 4;
 constexpr int WS_R = 128;
 constexpr int WS_SPIN = 1 << 21;          /* default try_wait attempts before giving up */
 
-/* A stage's records are written in PROD regions of WS_R / PROD slots, one
- * per producer warp; in region w the nf[w] records that are full-tier for
- * every consumer warp come first (slots 0.., in line order) and the nn[w]
- * others last (slots from the end downwards, in line order): consumers take
- * the first block without any tier test.  The order in which a bin sums its
- * lines is therefore a fixed function of the tile's lines. */
-constexpr int WS_MAX_PROD = 4;
 struct StageHdr {
     long long j0;          /* absolute first bin of the tile                */
     int jl;                /* job index                                     */
@@ -1087,10 +1028,6 @@ struct StageHdr {
     int flags;             /* 1 first stage of the tile, 2 last, 4 end,
                               8 the item is one slice of a split tile       */
     int item, tile;        /* work item and its tile                        */
-    int nf[WS_MAX_PROD];   /* all-full records of each producer region      */
-    int nn[WS_MAX_PROD];   /* other records of each producer region         */
-    int pair;              /* the stage's pair within its pack              */
-    int pad;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
@@ -1125,68 +1062,40 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
     return false;
 }
 
-/* packs of at most WS_MAX_PP pairs */
-constexpr int WS_MAX_PP = 4;
-
-/* shared-memory layout of voigt_ws_kernel for pp pairs per pack: the
- * stage ring and its headers and barriers, two staging buffers of WS_R
- * lines (one chunk each) per staged field, and a Kahan (sum, compensation)
- * pair per bin and pair of the pack */
-struct WsLayout {
-    size_t off_rec, off_hdr, off_bar, off_stg, off_gn, off_kahan, bytes;
-    int nf64;              /* staged FP64 fields per line */
-};
-
 template <int B, int CONS, int PROD, bool PREP>
-__host__ __device__ inline WsLayout ws_layout(int pp)
-{
-    WsLayout L;
-    const int W = 32 * B * CONS;
-    /* prep: nu and S, 1/width, y of every pair; on load: nu, E'', A, gamma, n */
-    L.nf64 = PREP ? 1 + 3 * pp : 5;
-    L.off_rec = 0;
-    L.off_hdr = L.off_rec + (size_t)WS_STAGES * WS_R * sizeof(RecV);
-    L.off_bar = L.off_hdr + (size_t)WS_STAGES * sizeof(StageHdr);
+struct WsSmem {
+    static constexpr int NP = PROD * 32;
+    static constexpr int W = 32 * B * CONS;
+    static constexpr int NF64 = PREP ? 4 : 5;
+    static constexpr size_t off_rec = 0;
+    static constexpr size_t off_hdr = off_rec + (size_t)WS_STAGES * WS_R * sizeof(RecV);
+    static constexpr size_t off_bar = off_hdr + (size_t)WS_STAGES * sizeof(StageHdr);
     /* mbarriers: full[WS_STAGES], empty[WS_STAGES], producers' own barrier,
      * consumers' own barrier */
-    L.off_stg = (L.off_bar + (size_t)(2 * WS_STAGES + 2) * sizeof(unsigned long long) + 15) & ~size_t(15);
-    L.off_gn = L.off_stg + (size_t)L.nf64 * 2 * WS_R * sizeof(double);
-    L.off_kahan = (L.off_gn + (PREP ? 0 : (size_t)2 * WS_R * sizeof(int)) + 15) & ~size_t(15);
-    L.bytes = L.off_kahan + (size_t)pp * 2 * W * sizeof(float);
-    return L;
-}
+    static constexpr size_t off_stg = off_bar + (size_t)(2 * WS_STAGES + 2) * sizeof(unsigned long long);
+    static constexpr size_t off_gn = off_stg + (size_t)NF64 * 2 * NP * sizeof(double);
+    static constexpr size_t off_kahan = (off_gn + (PREP ? 0 : (size_t)2 * NP * sizeof(int)) + 15) & ~size_t(15);
+    static constexpr size_t bytes = off_kahan + (size_t)2 * W * sizeof(float);
+};
 
-/* Packs (KArgs.pk_jobs): the pairs of a pack share the grid, the cutoff,
- * the window rule and the line list, so a tile finds the same lines for
- * all of them.  The producers stage each chunk of those lines once, find
- * each line's window in the tile once, and derive one stage of records per
- * pair from them (S, width and y are the pair's); the consumers add a
- * stage into the Kahan pairs of its pair.  A pair's bins sum its records in
- * the order they would have without the pack: results are bitwise those of
- * one pair per work item. */
 template <int B, int CONS, int PROD, bool PREP>
 __global__ void __launch_bounds__((CONS + PROD) * 32, CONS == 4 ? (B >= 8 ? 3 : 4) : 2)
 voigt_ws_kernel(const KArgs args)
 {
-    constexpr int NP = PROD * 32, W = 32 * B * CONS;
-    /* tier code 1 (full) for every consumer warp */
-    constexpr int kAllFull = 0x55555555 & ((1 << (2 * CONS)) - 1);
-    static_assert(WS_R % NP == 0 && WS_R / NP <= 2, "stage size and producer threads");
-    static_assert(PROD <= WS_MAX_PROD && CONS <= 8, "launch shape");
-    const int pp = args.pk_jobs ? args.pp : 1;
-    const WsLayout L = ws_layout<B, CONS, PROD, PREP>(pp);
-    const int R = args.lps;                      /* lines per stage (64 or 128)        */
-    const int SUB = R / NP;                      /* lines per producer thread per stage */
-    const int WR = R / PROD;                     /* records per producer region        */
+    typedef WsSmem<B, CONS, PROD, PREP> L;
+    constexpr int NP = L::NP, W = L::W;
+    constexpr int SUB = WS_R / NP;               /* lines per producer thread per stage */
+    static_assert(WS_R % NP == 0, "stage size must be a multiple of the producer threads");
     extern __shared__ __align__(16) unsigned char smem[];
-    RecV* s_rec = reinterpret_cast<RecV*>(smem + L.off_rec);
-    StageHdr* s_hdr = reinterpret_cast<StageHdr*>(smem + L.off_hdr);
-    unsigned long long* s_full = reinterpret_cast<unsigned long long*>(smem + L.off_bar);
+    RecV* s_rec = reinterpret_cast<RecV*>(smem + L::off_rec);
+    StageHdr* s_hdr = reinterpret_cast<StageHdr*>(smem + L::off_hdr);
+    unsigned long long* s_full = reinterpret_cast<unsigned long long*>(smem + L::off_bar);
     unsigned long long* s_empty = s_full + WS_STAGES;
     unsigned long long* s_pbar = s_empty + WS_STAGES;
-    double* s_f = reinterpret_cast<double*>(smem + L.off_stg);
-    int* s_gn = reinterpret_cast<int*>(smem + L.off_gn);
-    float* s_kahan = reinterpret_cast<float*>(smem + L.off_kahan);
+    double* s_f = reinterpret_cast<double*>(smem + L::off_stg);
+    int* s_gn = reinterpret_cast<int*>(smem + L::off_gn);
+    float* s_ks = reinterpret_cast<float*>(smem + L::off_kahan);
+    float* s_kc = s_ks + W;
     __shared__ int s_item;
     __shared__ long long s_lohi[2];
 
@@ -1218,7 +1127,6 @@ voigt_ws_kernel(const KArgs args)
             pph ^= 1;
             return ok;
         };
-        const size_t FS = (size_t)2 * WS_R;   /* staging entries per field */
         for (;;) {
             if (ptid == 0) s_item = atomicAdd(args.counter, 1);
             if (!psync()) { fail(); return; }
@@ -1238,19 +1146,13 @@ voigt_ws_kernel(const KArgs args)
                 sidx = item - __ldg(args.sl.prefix + tl);
                 ns = __ldg(args.sl.prefix + tl + 1) - __ldg(args.sl.prefix + tl);
             }
-            /* the tile's pack (a pack of one job without packs) */
-            int kl = 0, kh = args.njobs;
-            while (kh - kl > 1) { int m = (kl + kh) >> 1; if (__ldg(args.prefix + m) <= ti) kl = m; else kh = m; }
-            auto job_of = [&](int p) -> int {
-                return args.pk_jobs ? __ldg(args.pk_jobs + kl * pp + p) : (p == 0 ? kl : -1);
-            };
-            int npair = 1;
-            while (npair < pp && job_of(npair) >= 0) ++npair;
-            const gexs_job* Jp = args.jobs + job_of(0);
+            int jl = 0, jh = args.njobs;
+            while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
+            const gexs_job* Jp = args.jobs + jl;
             const gexs_job& J = *Jp;
             Tile T;
             T.J = Jp;
-            T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + kl)) * W;
+            T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * W;
             T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
             T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
             T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
@@ -1279,32 +1181,27 @@ voigt_ws_kernel(const KArgs args)
             if (!psync()) { fail(); return; }
             const int64_t lo = s_lohi[0];
             const int64_t hi = max((int64_t)s_lohi[1], lo);
-            const int nchunk = max(1, (int)((hi - lo + R - 1) / R));
-            /* chunk c of lines lo + c R .. into staging buffer c & 1; producer
-             * thread ptid stages and later reads lines sub * NP + ptid only */
-            auto issue = [&](int c) {
-                if (c < nchunk) {
-                    const size_t bo = (size_t)(c & 1) * WS_R;
-                    for (int sub = 0; sub < SUB; ++sub) {
-                        const int r = sub * NP + ptid;
-                        const int64_t i = lo + (int64_t)c * R + r;
-                        if (i >= hi) break;
-                        const size_t o = bo + r;
-                        cp_async8(s_f + o, J.lines.nu + i);
-                        if constexpr (PREP) {
-                            for (int p = 0; p < npair; ++p) {
-                                const double* pb = args.prep[job_of(p)];
-                                cp_async8(s_f + (1 + 3 * p) * FS + o, pb + i);
-                                cp_async8(s_f + (2 + 3 * p) * FS + o, pb + nl + i);
-                                cp_async8(s_f + (3 + 3 * p) * FS + o, pb + 2 * nl + i);
-                            }
-                        } else {
-                            cp_async8(s_f + FS + o, J.lines.elow + i);
-                            cp_async8(s_f + 2 * FS + o, J.lines.aif + i);
-                            cp_async4(s_gn + o, J.lines.gns + i);
-                            cp_async8(s_f + 3 * FS + o, J.lines.gamma + i);
-                            cp_async8(s_f + 4 * FS + o, J.lines.n + i);
-                        }
+            const int nchunk = max(1, (int)((hi - lo + WS_R - 1) / WS_R));
+            const int nsub = nchunk * SUB;
+            const double* pb = nullptr;
+            if constexpr (PREP) pb = args.prep[jl];
+            /* producer thread ptid stages and derives lines lo + u*NP + ptid;
+             * it reads only the staging slots it filled itself */
+            auto issue = [&](int u) {
+                const int64_t i = lo + (int64_t)u * NP + ptid;
+                const int o = (u & 1) * NP + ptid;
+                if (u < nsub && i < hi) {
+                    cp_async8(s_f + o, J.lines.nu + i);
+                    if constexpr (PREP) {
+                        cp_async8(s_f + 2 * NP + o, pb + i);
+                        cp_async8(s_f + 4 * NP + o, pb + nl + i);
+                        cp_async8(s_f + 6 * NP + o, pb + 2 * nl + i);
+                    } else {
+                        cp_async8(s_f + 2 * NP + o, J.lines.elow + i);
+                        cp_async8(s_f + 4 * NP + o, J.lines.aif + i);
+                        cp_async4(s_gn + o, J.lines.gns + i);
+                        cp_async8(s_f + 6 * NP + o, J.lines.gamma + i);
+                        cp_async8(s_f + 8 * NP + o, J.lines.n + i);
                     }
                 }
                 cp_async_commit();
@@ -1312,82 +1209,45 @@ voigt_ws_kernel(const KArgs args)
             issue(0);
             issue(1);
             for (int c = 0; c < nchunk; ++c) {
-                cp_async_wait<1>();                  /* chunk c has landed */
-                const int64_t pbase = lo + (int64_t)c * R;
-                const int nrec = (int)max((int64_t)0, min((int64_t)R, hi - pbase));
-                const size_t bo = (size_t)(c & 1) * WS_R;
-                /* each line's centre and window in the tile, for every pair */
-                double nuv[2], tcv[2];
-                int wab[2];
+                if (!mbar_wait(s_empty + st, ph, args.spin)) { fail(); return; }
+                const int64_t pbase = lo + (int64_t)c * WS_R;
+                const int nrec = (int)max((int64_t)0, min((int64_t)WS_R, hi - pbase));
+                RecV* rec = s_rec + st * WS_R;
 #pragma unroll
-                for (int sub = 0; sub < 2; ++sub) {
-                    nuv[sub] = 0.0; tcv[sub] = 0.0; wab[sub] = 0;
-                    if (sub >= SUB) continue;
+                for (int sub = 0; sub < SUB; ++sub) {
+                    const int u = c * SUB + sub;
+                    const int o = (u & 1) * NP + ptid;
+                    cp_async_wait<1>();
                     const int r = sub * NP + ptid;
                     if (r < nrec) {
-                        const double nu0 = s_f[bo + r];
-                        const double nu = nu0 == 0.0 ? 1e-6 : nu0;
-                        const double tc = dmul(dsub(nu, T.f0), T.inv_dnu);
-                        int a, b;
-                        tile_window(T, nu, tc, &a, &b);
-                        nuv[sub] = nu; tcv[sub] = tc; wab[sub] = pack2(a, b);
-                    }
-                }
-                for (int p = 0; p < npair; ++p) {
-                    if (!mbar_wait(s_empty + st, ph, args.spin)) { fail(); return; }
-                    const int jp = job_of(p);
-                    /* the pairs share the grid: only the job changes */
-                    T.J = args.jobs + jp;
-                    const gexs_job& Jq = *T.J;
-                    /* this producer warp's region of the stage */
-                    RecV* reg = s_rec + st * WS_R + pw * WR;
-                    int nf = 0, nn = 0;
-#pragma unroll
-                    for (int sub = 0; sub < 2; ++sub) {
-                        if (sub >= SUB) break;
-                        const int r = sub * NP + ptid;
-                        const size_t o = bo + r;
-                        const bool valid = r < nrec;
-                        RecV rr;
-                        if (valid) {
-                            LineQ lq;
-                            if constexpr (PREP) {
-                                lq.nu = nuv[sub];
-                                lq.S = s_f[(1 + 3 * p) * FS + o];
-                                lq.invw = s_f[(2 + 3 * p) * FS + o];
-                                lq.y = s_f[(3 + 3 * p) * FS + o];
-                            } else {
-                                RawLine Lr;
-                                Lr.nu = s_f[o]; Lr.elow = s_f[FS + o]; Lr.aif = s_f[2 * FS + o];
-                                Lr.g = s_gn[o]; Lr.gam = s_f[3 * FS + o]; Lr.nexp = s_f[4 * FS + o];
-                                lq = line_quantities<true>(Jq, Lr);
-                            }
-                            Derived<PK_VOIGT> d = derive_line_win<PK_VOIGT>(T, lq, 10.5, tcv[sub],
-                                                                           lo16(wab[sub]), hi16(wab[sub]));
-                            make_rec<PK_VOIGT, B, CONS>(rr, d, Jq, T);
+                        LineQ lq;
+                        if constexpr (PREP) {
+                            const double nu = s_f[o];
+                            lq.nu = nu == 0.0 ? 1e-6 : nu;
+                            lq.S = s_f[2 * NP + o]; lq.invw = s_f[4 * NP + o]; lq.y = s_f[6 * NP + o];
+                        } else {
+                            RawLine Lr;
+                            Lr.nu = s_f[o]; Lr.elow = s_f[2 * NP + o]; Lr.aif = s_f[4 * NP + o];
+                            Lr.g = s_gn[o]; Lr.gam = s_f[6 * NP + o]; Lr.nexp = s_f[8 * NP + o];
+                            lq = line_quantities<true>(J, Lr);
                         }
-                        const bool full = valid && rr.tiers == kAllFull;
-                        const unsigned bf = __ballot_sync(0xffffffffu, full);
-                        const unsigned bn = __ballot_sync(0xffffffffu, valid && !full);
-                        const unsigned below = (1u << lane) - 1u;
-                        if (full) reg[nf + __popc(bf & below)] = rr;
-                        else if (valid) reg[WR - 1 - (nn + __popc(bn & below))] = rr;
-                        nf += __popc(bf);
-                        nn += __popc(bn);
+                        Derived<PK_VOIGT> d = derive_line_body<PK_VOIGT>(T, lq, 10.5);
+                        RecV rr;
+                        make_rec<PK_VOIGT, B, CONS>(rr, d, J, T);
+                        rec[r] = rr;
                     }
-                    if (lane == 0) { s_hdr[st].nf[pw] = nf; s_hdr[st].nn[pw] = nn; }
-                    if (ptid == 0) {
-                        StageHdr& h = s_hdr[st];
-                        h.j0 = T.j0; h.jl = jp; h.jn = T.jn; h.nrec = nrec;
-                        h.flags = (c == 0 ? 1 : 0) | (c == nchunk - 1 ? 2 : 0) | (ns > 1 ? 8 : 0);
-                        h.item = item;
-                        h.tile = ti;
-                        h.pair = p;
-                    }
-                    mbar_arrive(s_full + st);
-                    if (++st == WS_STAGES) { st = 0; ph ^= 1; }
+                    issue(u + 2);
                 }
-                issue(c + 2);                        /* into this chunk's buffer */
+                if (ptid == 0) {
+                    StageHdr h;
+                    h.j0 = T.j0; h.jl = jl; h.jn = T.jn; h.nrec = nrec;
+                    h.flags = (c == 0 ? 1 : 0) | (c == nchunk - 1 ? 2 : 0) | (ns > 1 ? 8 : 0);
+                    h.item = item;
+                    h.tile = ti;
+                    s_hdr[st] = h;
+                }
+                mbar_arrive(s_full + st);
+                if (++st == WS_STAGES) { st = 0; ph ^= 1; }
             }
             cp_async_wait<0>();
             /* every producer is past s_item and s_lohi */
@@ -1415,9 +1275,6 @@ voigt_ws_kernel(const KArgs args)
         if (!mbar_wait(s_full + st, ph, args.spin)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
         const StageHdr h = s_hdr[st];
         if (h.flags & 4) return;
-        /* Kahan pairs of this stage's pair; each lane owns its bins */
-        float* s_ks = s_kahan + (size_t)h.pair * 2 * W;
-        float* s_kc = s_ks + W;
         if (h.flags & 1) {
 #pragma unroll
             for (int k = 0; k < B; ++k) {
@@ -1426,16 +1283,7 @@ voigt_ws_kernel(const KArgs args)
             }
         }
         const RecV* rec = s_rec + st * WS_R;
-        {
-            const float lw = (float)(warp * 32 * B + lane);
-            const float2 lw2 = make_float2(lw, lw);
-#pragma unroll
-            for (int w = 0; w < PROD; ++w) {
-                const RecV* reg = rec + w * WR;
-                lines_voigt_allfull<B>(reg, h.nf[w], lw2, part);
-                lines_voigt_f32<B>(reg + WR - h.nn[w], h.nn[w], warp, lane, part);
-            }
-        }
+        lines_voigt_f32<B>(rec, h.nrec, warp, lane, part);
 #pragma unroll
         for (int k = 0; k < B; ++k) {
             const int t = warp * 32 * B + lane + 32 * k;
@@ -1458,15 +1306,14 @@ voigt_ws_kernel(const KArgs args)
                 }
             }
         } else if (h.flags & 2) {
-            /* one slice of a split tile: its partial row of this pair, then a
-             * ticket of (tile, pair); the last slice to finish adds the rows
-             * in slice order */
+            /* one slice of a split tile: its partial row, then a ticket; the
+             * last slice to finish adds the rows in slice order */
             const gexs_job& J = args.jobs[h.jl];
             double* out = J.out;
             const int base = args.sl.prefix[h.tile];
             const int ns = args.sl.prefix[h.tile + 1] - base;
             const int rb = args.sl.rowbase[h.tile];
-            double* row = args.sl.rows + ((size_t)(rb + (h.item - base)) * pp + h.pair) * W;
+            double* row = args.sl.rows + (size_t)(rb + (h.item - base)) * W;
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const int t = warp * 32 * B + lane + 32 * k;
@@ -1474,7 +1321,7 @@ voigt_ws_kernel(const KArgs args)
             }
             __threadfence();
             if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
-            if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile * pp + h.pair, 1) == ns - 1;
+            if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile, 1) == ns - 1;
             if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
             if (s_last) {
                 __threadfence();
@@ -1483,8 +1330,7 @@ voigt_ws_kernel(const KArgs args)
                     const int t = warp * 32 * B + lane + 32 * k;
                     if (t < h.jn) {
                         double v = 0.0;
-                        for (int q = 0; q < ns; ++q)
-                            v += __ldcg(args.sl.rows + ((size_t)(rb + q) * pp + h.pair) * W + t);
+                        for (int q = 0; q < ns; ++q) v += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
                         const int64_t j = h.j0 + t;
                         out[j] = J.accumulate ? out[j] + v : v;
                     }
@@ -1736,7 +1582,7 @@ static cudaError_t launch_ws_one(const KArgs& a, int ctas_per_sm, int nsm, cudaS
 {
     constexpr int PROD = 2;
     auto kern = voigt_ws_kernel<B, CONS, PROD, PREP>;
-    const size_t smem = ws_layout<B, CONS, PROD, PREP>(a.pk_jobs ? a.pp : 1).bytes;
+    const size_t smem = WsSmem<B, CONS, PROD, PREP>::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
@@ -1840,26 +1686,13 @@ static cudaError_t launch_pk(int prec, const KArgs& a, const gexs_launch_cfg& cf
 {
     const bool prep = a.prep != nullptr;
     if (prec == GEXS_FP32) {
-        /* the FP32 Voigt region-I kernel walks the tiles of packs of pairs
-         * (one job per pack without packs); every other kernel, the core
-         * kernel included, walks the tiles of the jobs */
-        KArgs r = a;
-        if (PK == PK_VOIGT && a.pk_jobs) {
-            r.prefix = a.pk_prefix; r.njobs = a.npacks; r.nitems = a.pk_nitems;
-        } else {
-            r.pk_jobs = nullptr; r.pp = 1;
-        }
-        cudaError_t e = prep ? launch_cfg<PK, GEXS_FP32, true>(r, cfg, nsm, st)
-                             : launch_cfg<PK, GEXS_FP32, false>(r, cfg, nsm, st);
+        cudaError_t e = prep ? launch_cfg<PK, GEXS_FP32, true>(a, cfg, nsm, st)
+                             : launch_cfg<PK, GEXS_FP32, false>(a, cfg, nsm, st);
         if (PK != PK_VOIGT || e != cudaSuccess) return e;
-        KArgs c = a;
-        c.pk_jobs = nullptr; c.pp = 1;
-        return prep ? launch_core<true>(c, nsm, st) : launch_core<false>(c, nsm, st);
+        return prep ? launch_core<true>(a, nsm, st) : launch_core<false>(a, nsm, st);
     }
-    KArgs a64 = a;
-    a64.pk_jobs = nullptr; a64.pp = 1;
-    return prep ? launch_cfg<PK, GEXS_FP64, true>(a64, cfg, nsm, st)
-                : launch_cfg<PK, GEXS_FP64, false>(a64, cfg, nsm, st);
+    return prep ? launch_cfg<PK, GEXS_FP64, true>(a, cfg, nsm, st)
+                : launch_cfg<PK, GEXS_FP64, false>(a, cfg, nsm, st);
 }
 
 /* defined one per translation unit */

@@ -135,8 +135,9 @@ def _cfg(cfg):
         return None
     if isinstance(cfg, capi.GexsLaunchCfg):
         return C.byref(cfg)
-    vals = list(cfg) + [0] * (7 - len(cfg))
-    return C.byref(capi.GexsLaunchCfg(*vals[:7]))
+    b, w, c = cfg[:3]
+    return C.byref(capi.GexsLaunchCfg(b, w, c, cfg[3] if len(cfg) > 3 else 0,
+                                      cfg[4] if len(cfg) > 4 else 0))
 
 
 class Batch:
@@ -206,8 +207,7 @@ class Context:
         ms = C.c_float()
         check(lib().gexs_autotune(self.h, arr, len(arr), C.byref(best), C.byref(ms)),
               "gexs_autotune")
-        return (best.bins_per_lane, best.warps, best.ctas_per_sm, best.flags, 0, best.pairs,
-                best.lines_per_stage), float(ms.value)
+        return (best.bins_per_lane, best.warps, best.ctas_per_sm), float(ms.value)
 
     def partition(self, energy, g, temps):
         temps = np.ascontiguousarray(temps, dtype=np.float64)

@@ -116,6 +116,8 @@ double B200ExomolReader::ComputePartition(double temperature)
 gexs_lines B200ExomolReader::device_lines() const
 {
     gexs_lines l;
+    std::memset(&l, 0, sizeof(l));
+    l.format = GEXS_LINES_FP64;
     l.nu = lines_.nu; l.elow = lines_.elow; l.aif = lines_.aif; l.gns = lines_.gns;
     l.gamma = lines_.gamma; l.n = lines_.n; l.count = lines_.count;
     return l;

@@ -133,6 +133,10 @@ struct gexs_server {
     std::deque<Req*> pending;
     std::unordered_map<uint64_t, Req*> reqs;
     std::vector<Batch> running;
+    /* a batch's event and the requests of that batch not yet fetched: the
+     * last waiter to fetch destroys it (waiters remove their request from
+     * `reqs` before they use the event, so `reqs` cannot tell) */
+    std::unordered_map<cudaEvent_t, int> ev_refs;
     size_t inflight_bytes = 0;
     int inflight = 0;
     uint64_t next_id = 1;
@@ -270,6 +274,7 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
             r->done = b.ev;
         }
     }
+    if (!status) s->ev_refs[b.ev] = (int)adm.size();
     if (status) {
         /* nothing of this batch is read back: wait for its work before the
          * slot and the outputs are reused */
@@ -417,7 +422,8 @@ int gexs_server_destroy(gexs_server* s)
         if (r->d_out) cudaFree(r->d_out);
         delete r;
     }
-    for (Batch& b : s->running) cudaEventDestroy(b.ev);
+    /* every batch event still referenced, running or finished unfetched */
+    for (auto& kv : s->ev_refs) cudaEventDestroy(kv.first);
     for (List& L : s->lists) {
         cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
         cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.se); cudaFree(L.sg); cudaFree(L.d_qtab);
@@ -596,7 +602,7 @@ int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_
         if (e != cudaSuccess && !status) status = gexs::cuda_error(e, "result copy");
         r->d_out = nullptr;
     }
-    bool last_of_batch = true;
+    bool last_of_batch = false;
     {
         std::lock_guard<std::mutex> g(s->mu);
         s->inflight--;
@@ -604,9 +610,13 @@ int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_
         r->info.fetched_ms = s->now_ms();
         r->info.status = status;
         s->kick = true;
-        if (r->done)
-            for (auto& kv : s->reqs)
-                if (kv.second->done == r->done) { last_of_batch = false; break; }
+        if (r->done) {
+            auto e = s->ev_refs.find(r->done);
+            if (e != s->ev_refs.end() && --e->second == 0) {
+                s->ev_refs.erase(e);
+                last_of_batch = true;
+            }
+        }
     }
     if (r->done && last_of_batch) cudaEventDestroy(r->done);
     if (info) *info = r->info;

@@ -171,12 +171,6 @@ typedef struct gexs_launch_cfg {
                                 Voigt pipeline before it gives up and
                                 flags GEXS_ERR_KERNEL (0 = 2^21, about
                                 0.5 s of back-off per wait)           */
-    int32_t pairs;           /* FP32 Voigt: jobs (T, P pairs) of one grid
-                                and one line list evaluated together per
-                                tile, sharing each staged chunk of lines
-                                and its windows: 1, 2 or 4 (0 = 1)    */
-    int32_t lines_per_stage; /* FP32 Voigt: lines per pipeline stage,
-                                64 or 128 (0 = 128)                   */
 } gexs_launch_cfg;
 
 /* derive S(T), width and y of every line in the tile loader instead of
@@ -374,11 +368,10 @@ int gexs_batch_capture(gexs_batch* b, void* stream);  /* build the graph   */
 int gexs_batch_replay(gexs_batch* b, void* stream);   /* launch the graph  */
 int gexs_batch_destroy(gexs_batch* b);
 
-/* Pick the launch shape for these jobs by timing each candidate (CUDA
- * events) on the jobs themselves: tile width (bins per lane x warps), and
- * for the FP32 Voigt form lines per stage and pairs per CTA.  Writes the
- * winner to *best and records it as the context default for the jobs'
- * profile and precision; h_ms (may be NULL) gets the winner's time. */
+/* Pick bins_per_lane / warps / ctas_per_sm for these jobs by timing each
+ * candidate (CUDA events) on the jobs themselves.  Writes the winner to
+ * *best and records it as the context default for the jobs' profile and
+ * precision; h_ms (may be NULL) gets the winner's time. */
 int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
                   gexs_launch_cfg* best, float* h_ms);
 

@@ -63,8 +63,11 @@ def test_multi_equals_single_device_and_oracle(prec):
     for devices in ([0, 0], [0, 0, 0], [0] * 6):
         multi = _drive(Manager(capi.VOIGT, convention=capi.CONV_PHYSICAL, precision=prec,
                                memory_bytes=1 << 27, devices=devices), L, chunks, zero)
-        for s, m in zip(single, multi):
-            np.testing.assert_array_equal(m, s)
+        for k, (s, m) in enumerate(zip(single, multi)):
+            bad = np.flatnonzero(m != s)
+            assert bad.size == 0, "devices %d pair %d: %d bins differ, first %s: %r vs %r" % (
+                len(devices), k, bad.size, bad[:4].tolist(), m[bad[:4]].tolist(),
+                s[bad[:4]].tolist())
     initial = np.linspace(0.0, 1e-22, G)
     single = _drive(Manager(capi.VOIGT, 0, capi.CONV_PHYSICAL, prec, 1 << 28), L, chunks,
                     initial)

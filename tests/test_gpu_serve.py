@@ -56,6 +56,36 @@ def test_alone_equals_mixed(served):
     assert max(sizes) > 1, "requests submitted together were never batched"
 
 
+def test_concurrent_waiters_of_one_batch(served):
+    """Many threads fetch the requests of the same batches at once, in an
+    order unrelated to submission: each gets its own result (equal to the
+    request run alone) and the batch's completion event outlives every
+    waiter that still uses it."""
+    srv, lid, lid_dop = served
+    reqs = _requests(lid, lid_dop, n=48, seed=11)
+    alone = [srv.wait(srv.submit(r), r.grid_points)[0] for r in reqs]
+    for _ in range(3):
+        tickets = [srv.submit(r) for r in reqs]
+        got = [None] * len(reqs)
+        errors = []
+
+        def fetch(idx):
+            try:
+                for i in idx:
+                    got[i] = srv.wait(tickets[i], reqs[i].grid_points)[0]
+            except Exception as e:  # pragma: no cover
+                errors.append(e)
+        order = np.random.Generator(np.random.PCG64(7)).permutation(len(reqs))
+        threads = [threading.Thread(target=fetch, args=(order[k::12],)) for k in range(12)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        assert not errors, errors[0]
+        for a, b in zip(alone, got):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_served_results_match_oracle(served, small_states, small_lines):
     from oracle import pyoracle as po
     srv, lid, lid_dop = served
