@@ -6,11 +6,14 @@ through the BaseManager C view, as BaseProfile drives it
 Every run here has one GPU, so the shards are several entries of device 0
 (each its own manager, context and streams; nothing waits on another
 shard).  Cuts fall on multiples of 4096 bins, so each shard computes the
-tiles of a single launch: with the zero initial grid BaseProfile passes,
-the sharded results equal the one-device manager's bit for bit, in the FP64
-and FP32 forms.  A non-zero initial grid is added once on the host, after
-the devices' sums (the one-device manager adds the sums onto it), so there
-the two agree to one rounding (1e-15 relative).  The FP64 form matches the
+tiles of a single launch: for one chunk and the zero initial grid
+BaseProfile passes, the sharded results equal the one-device manager's bit
+for bit, in the FP64 and FP32 forms.  Each chunk is cut for its own lines,
+so a bin that two chunks reach may belong to different devices in the two;
+the host then adds the devices' sums, where one device adds the second
+chunk onto the first: the association differs, one rounding per chunk
+(1e-15 relative).  A non-zero initial grid is likewise added once on the
+host, after the devices' sums.  The FP64 form matches the
 FP64 oracle within 1e-10 per bin.  A shard may be empty (more shards than
 the band needs) without changing the result.
 """
@@ -59,15 +62,21 @@ def test_multi_equals_single_device_and_oracle(prec):
     L = synth.make_lines(st, 60000, 150.0, 5900.0, 2007, broadening_seed=3007)
     chunks = [(0, 25000), (25000, 60000)]
     zero = np.zeros(G)
+    one = [(0, 60000)]
+    single1 = _drive(Manager(capi.VOIGT, 0, capi.CONV_PHYSICAL, prec, 1 << 28), L, one, zero)
     single = _drive(Manager(capi.VOIGT, 0, capi.CONV_PHYSICAL, prec, 1 << 28), L, chunks, zero)
     for devices in ([0, 0], [0, 0, 0], [0] * 6):
-        multi = _drive(Manager(capi.VOIGT, convention=capi.CONV_PHYSICAL, precision=prec,
-                               memory_bytes=1 << 27, devices=devices), L, chunks, zero)
-        for k, (s, m) in enumerate(zip(single, multi)):
+        kw = dict(convention=capi.CONV_PHYSICAL, precision=prec, memory_bytes=1 << 27,
+                  devices=devices)
+        multi1 = _drive(Manager(capi.VOIGT, **kw), L, one, zero)
+        for k, (s, m) in enumerate(zip(single1, multi1)):
             bad = np.flatnonzero(m != s)
             assert bad.size == 0, "devices %d pair %d: %d bins differ, first %s: %r vs %r" % (
                 len(devices), k, bad.size, bad[:4].tolist(), m[bad[:4]].tolist(),
                 s[bad[:4]].tolist())
+        multi = _drive(Manager(capi.VOIGT, **kw), L, chunks, zero)
+        for s, m in zip(single, multi):
+            assert np.all(np.abs(m - s) <= 1e-15 * np.abs(s))
     initial = np.linspace(0.0, 1e-22, G)
     single = _drive(Manager(capi.VOIGT, 0, capi.CONV_PHYSICAL, prec, 1 << 28), L, chunks,
                     initial)
