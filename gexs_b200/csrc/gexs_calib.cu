@@ -39,7 +39,17 @@ __global__ void __launch_bounds__(256) dfma_probe(double* sink, int iters, doubl
     if (s == 12345.678) sink[blockIdx.x] = s;
 }
 
-/* reciprocal approximations (one MUFU op each) on independent chains */
+/* reciprocal approximations (one MUFU op each) on independent chains.
+ * Each step is r(1 + x/2): the FMA keeps the compiler from folding a
+ * reciprocal of a reciprocal and costs an eighth of a MUFU op's issue
+ * time on the FP32 pipe. */
+__device__ __forceinline__ float rcp_step(float x)
+{
+    float r;
+    asm volatile("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fmaf(x, 0.5f, 1.0f)));
+    return r;
+}
+
 __global__ void __launch_bounds__(256) rcp_probe(float* sink, int iters)
 {
     float x0 = 1.f + threadIdx.x * 1e-7f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
@@ -47,8 +57,8 @@ __global__ void __launch_bounds__(256) rcp_probe(float* sink, int iters)
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
         for (int u = 0; u < 16; ++u) {
-            x0 = rcp_approx(x0); x1 = rcp_approx(x1); x2 = rcp_approx(x2); x3 = rcp_approx(x3);
-            x4 = rcp_approx(x4); x5 = rcp_approx(x5); x6 = rcp_approx(x6); x7 = rcp_approx(x7);
+            x0 = rcp_step(x0); x1 = rcp_step(x1); x2 = rcp_step(x2); x3 = rcp_step(x3);
+            x4 = rcp_step(x4); x5 = rcp_step(x5); x6 = rcp_step(x6); x7 = rcp_step(x7);
         }
     }
     float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
