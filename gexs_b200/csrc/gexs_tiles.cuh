@@ -185,7 +185,7 @@ __device__ __forceinline__ void tile_window(const Tile& T, double nu, double tc,
     else if (tcen > 0 && in(tcen - 1)) anchor = tcen - 1;
     else if (tcen + 1 < T.jn && in(tcen + 1)) anchor = tcen + 1;
     if (anchor < 0) { *pa = *pb = 0; return; }
-    double w = cut / J.dnu;
+    double w = cut * T.inv_dnu;   /* guesses only: first_true finds the ends */
     int gl = (int)fmin(fmax(ceil(tc - w), 0.0), (double)anchor);
     int gr = (int)fmin(fmax(floor(tc + w) + 1.0, (double)anchor), (double)T.jn);
     *pa = first_true(0, anchor, gl, [&](int t) { return in(t); });
@@ -194,16 +194,20 @@ __device__ __forceinline__ void tile_window(const Tile& T, double nu, double tc,
 
 /* bins of [wa, wb) (a sub-range of the tile) where dist-predicate `in`
  * holds; `in` must be true on one contiguous interval around the line
- * centre.  d_thr is an estimate of the distance limit for the guesses. */
+ * centre.  The predicate can only hold where (dist - off) * invw <= xthr;
+ * the nearest bin's distance decides that without a division (a
+ * conservative test: `in` takes the exact decisions), and the guesses for
+ * the interval's ends come from the same limit. */
 template <typename P>
 __device__ __forceinline__ int centered(const Tile& T, int wa, int wb, double nu, double tc,
-                                        double d_thr, const P& in)
+                                        double xthr, double invw, double off, const P& in)
 {
-    if (wa >= wb || !(d_thr >= 0.0)) return 0;
+    if (wa >= wb || !(xthr >= 0.0)) return 0;
     double fa = grid_f(T.J->nu_start, T.J->dnu, T.j0 + wa);
     double fb = grid_f(T.J->nu_start, T.J->dnu, T.j0 + wb - 1);
     double dmin = nu < fa ? fa - nu : (nu > fb ? nu - fb : 0.0);
-    if (dmin > d_thr * (1.0 + 1e-9) + 1e-300) return 0;
+    if ((dmin - off) * invw > xthr * (1.0 + 1e-9) + 1e-300) return 0;
+    const double d_thr = xthr / invw + off;
     int tcen = (int)fmin(fmax(rint(tc), (double)wa), (double)(wb - 1));
     int anchor = -1;
     if (in(tcen)) anchor = tcen;
@@ -279,20 +283,20 @@ __device__ __forceinline__ Derived<PK> derive_line_body(const Tile& T, const Lin
     auto xof = [&](int tt) { return dmul(fabs(dsub(grid_f(nu_s, dnu, j0 + tt), nu)), invw); };
     if constexpr (PK == PK_VOIGT) {
         /* region tests of compute/CPU/profiles.cpp:17,24,31 */
-        d.c1 = centered(T, a, b, nu, d.tc, (15.0 - y) / invw,
+        d.c1 = centered(T, a, b, nu, d.tc, 15.0 - y, invw, 0.0,
                         [&](int tt) { return dadd(xof(tt), y) < 15.0; });
         if (lo16(d.c1) < hi16(d.c1)) {
-            d.c2 = centered(T, lo16(d.c1), hi16(d.c1), nu, d.tc, (5.5 - y) / invw,
+            d.c2 = centered(T, lo16(d.c1), hi16(d.c1), nu, d.tc, 5.5 - y, invw, 0.0,
                             [&](int tt) { return dadd(xof(tt), y) < 5.5; });
             if (lo16(d.c2) < hi16(d.c2))
-                d.c3 = centered(T, lo16(d.c2), hi16(d.c2), nu, d.tc, ((y + 0.176) / 0.195) / invw,
+                d.c3 = centered(T, lo16(d.c2), hi16(d.c2), nu, d.tc, (y + 0.176) / 0.195, invw, 0.0,
                                 [&](int tt) { return y >= dsub(dmul(0.195, xof(tt)), 0.176); });
         }
     } else if constexpr (PK == PK_ERF) {
         /* bins whose lower erf argument is <= zthr; beyond it both erfc
          * terms underflow to exactly zero */
         const double h = 0.5 * dnu;
-        d.c1 = centered(T, a, b, nu, d.tc, zthr / invw + h,
+        d.c1 = centered(T, a, b, nu, d.tc, zthr, invw, h,
                         [&](int tt) {
                             double dist = fabs(dsub(grid_f(nu_s, dnu, j0 + tt), nu));
                             return dmul(invw, dsub(dist, h)) <= zthr;

@@ -6,10 +6,12 @@
  *      requests marked done (waiters are woken);
  *   2. pending requests are admitted in arrival order while their output
  *      grids fit in the HBM budget and the in-flight cap allows;
- *   3. the admitted group gets Q(T) from the resident states (partition
- *      kernel on the worker's own stream), stream-ordered output buffers
- *      (cudaMallocAsync) and one gexs_run launch on the next stream of the
- *      pool, followed by an event.
+ *   3. the admitted group gets Q(T) from the resident table of its list
+ *      (or the partition kernel on the worker's own stream for temperatures
+ *      outside it), stream-ordered output buffers from the server's own
+ *      memory pool (cudaMallocFromPoolAsync; freed pages stay mapped) and
+ *      one gexs_run launch on the next stream of the server, followed by an
+ *      event.
  * Nothing on this path synchronises the device (no cudaMalloc/cudaFree),
  * so a new batch starts while earlier ones still run.  A request's output
  * is released when the caller fetches it (gexs_server_wait), which frees
@@ -121,6 +123,10 @@ struct gexs_server {
     int* d_errs = nullptr;
     int* h_errs = nullptr;
     std::vector<int> free_slots;
+    /* request outputs: a pool of the server's own that keeps freed memory
+     * mapped (admission bounds what it holds), so a request never waits
+     * for pages the previous one gave back */
+    cudaMemPool_t out_pool = nullptr;
 
     /* a deque: adding a list never moves the others, which the worker
      * reads without the lock while it launches */
@@ -235,7 +241,10 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
             j.lines.nu = L.nu; j.lines.elow = L.elow; j.lines.aif = L.aif; j.lines.gns = L.gns;
             j.lines.gamma = L.gamma; j.lines.n = L.n; j.lines.count = L.count;
             void* d = nullptr;
-            if (cudaMallocAsync(&d, r->bytes, st) != cudaSuccess) { status = GEXS_ERR_OOM; break; }
+            if (cudaMallocFromPoolAsync(&d, r->bytes, s->out_pool, st) != cudaSuccess) {
+                status = GEXS_ERR_OOM;
+                break;
+            }
             r->d_out = (double*)d;
             j.out = r->d_out;
             r->job = j;
@@ -401,6 +410,19 @@ int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int stre
               cudaMallocHost(&s->h_errs, sizeof(int) * s->max_inflight) == cudaSuccess;
     for (int i = s->max_inflight - 1; ok && i >= 0; --i) s->free_slots.push_back(i);
     if (!ok) { gexs_server_destroy(s); return gexs::set_error(GEXS_ERR_OOM, "server buffers"); }
+    {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        uint64_t keep = UINT64_MAX;
+        if (cudaMemPoolCreate(&s->out_pool, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(s->out_pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            gexs_server_destroy(s);
+            return gexs::set_error(GEXS_ERR_CUDA, "server output pool");
+        }
+    }
     s->worker = std::thread(worker_loop, s);
     *out = s;
     return GEXS_OK;
@@ -434,6 +456,7 @@ int gexs_server_destroy(gexs_server* s)
     cudaFree(s->d_betas); cudaFree(s->d_partial); cudaFree(s->d_q);
     cudaFree(s->d_errs);
     if (s->h_errs) cudaFreeHost(s->h_errs);
+    if (s->out_pool) cudaMemPoolDestroy(s->out_pool);
     gexs_ctx_destroy(s->ctx);
     delete s;
     return GEXS_OK;
