@@ -555,6 +555,19 @@ def serve_bench(torch, dev, local_rank, args):
                                   cutoff=CUT)
 
     reqs = [draw() for _ in range(args.serve_requests)]
+    # evaluations of the request set, counted on the generated copies, which
+    # are then freed: the server's budget (0.9 of the memory free when it was
+    # created) must not also cover them
+    ctx = Context(local_rank)
+    ev = 0
+    for li, rq in reqs:
+        j = Job(keep[li], torch.empty(1, dtype=torch.float64, device=dev),
+                convention=capi.CONV_PHYSICAL, profile=rq.profile, temperature=rq.temperature,
+                pressure=rq.pressure, partition=1.0, mass=lists[li][1], nu_start=rq.nu_start,
+                dnu=rq.dnu, grid_points=rq.grid_points, cutoff=CUT, n_points=rq.grid_points)
+        ev += ctx.count_evals([j])[0]
+    del keep, ctx, j
+    torch.cuda.empty_cache()
 
     def run(rate, seed):
         n = len(reqs)
@@ -597,14 +610,6 @@ def serve_bench(torch, dev, local_rank, args):
     for _, rq in reqs:
         srv.wait(srv.submit(rq), rq.grid_points)
     service = (time.perf_counter() - t0) / len(reqs)
-    ctx = Context(local_rank)
-    ev = 0
-    for li, rq in reqs:
-        j = Job(keep[li], torch.empty(1, dtype=torch.float64, device=dev),
-                convention=capi.CONV_PHYSICAL, profile=rq.profile, temperature=rq.temperature,
-                pressure=rq.pressure, partition=1.0, mass=lists[li][1], nu_start=rq.nu_start,
-                dnu=rq.dnu, grid_points=rq.grid_points, cutoff=CUT, n_points=rq.grid_points)
-        ev += ctx.count_evals([j])[0]
     rates = []
     for k, load in enumerate(args.serve_loads):
         rate = load / service

@@ -85,6 +85,7 @@ struct gexs_ctx {
 namespace gexs {
 int ctx_device(gexs_ctx* c) { return c->device; }
 int ctx_sm_count(gexs_ctx* c) { return c->nsm; }
+cudaMemPool_t ctx_pool(gexs_ctx* c) { return c->pool; }
 }  // namespace gexs
 
 static gexs_launch_cfg default_cfg(int pk, int prec)
@@ -453,6 +454,24 @@ int gexs_run(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_c
 }
 
 }  // extern "C"
+
+int gexs::run_scratch_bytes(gexs_ctx* ctx, const gexs_job* jobs, int njobs,
+                            const gexs_launch_cfg* cfg, size_t* bytes)
+{
+    if (!ctx || !bytes) return set_error(GEXS_ERR_INVALID, "arguments");
+    std::vector<Group> groups;
+    std::vector<gexs_launch_cfg> cfgs;
+    int st = build_groups(jobs, njobs, cfg, ctx, groups, cfgs);
+    if (st) return st;
+    size_t total = 0;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        if (groups[gi].nitems == 0) continue;
+        const bool prep = !(cfgs[gi].flags & GEXS_LAUNCH_DERIVE_ON_LOAD);
+        total += group_layout(groups[gi], prep, cfgs[gi]).bytes;
+    }
+    *bytes = total;
+    return GEXS_OK;
+}
 
 int gexs::run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
                    void* stream, int* d_err)

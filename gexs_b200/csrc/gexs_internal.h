@@ -76,9 +76,16 @@ cudaError_t take_word(int* word, int* out, cudaStream_t st);
 int run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
              void* stream, int* d_err);
 
-/* context accessors (gexs_capi.cu) */
+/* device scratch run_jobs takes from the context's pool for these jobs
+ * (launch tables, per-job prep arrays, line-slice rows), in bytes */
+int run_scratch_bytes(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg,
+                      size_t* bytes);
+
+/* context accessors (gexs_capi.cu); ctx_pool may be NULL (then the
+ * device's default pool serves the context) */
 int ctx_device(gexs_ctx* c);
 int ctx_sm_count(gexs_ctx* c);
+cudaMemPool_t ctx_pool(gexs_ctx* c);
 
 /* error reporting (gexs_capi.cu): thread-local message, returns status */
 int set_error(int status, const std::string& msg);

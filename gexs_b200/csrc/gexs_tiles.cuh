@@ -661,6 +661,103 @@ __device__ __forceinline__ void voigt_full4(const RecV* __restrict__ r, float2 l
     voigt_full2<B>(q[2], q[3], lw2, part);
 }
 
+/* Record-split form of the FP32 Voigt loop: every consumer warp covers
+ * the whole tile (lane l owns bins l + 32k, k < B*CONS) and takes every
+ * CONS-th record of a stage.  A record's constants are loaded once per
+ * tile instead of once per warp, and its B*CONS/2 bin pairs are
+ * independent chains.  Tier bits stay per quarter of 32*B bins (quarter q
+ * = the bins a warp owns in the bins-split form): quarter q of a lane is
+ * pairs q*B/2 .. q*B/2 + B/2 - 1. */
+template <int B, int Q, int NPAIR>
+__device__ __forceinline__ void voigt_quarter(const RecV& q, int tier, int lane, float2 n2,
+                                              float2 (&part)[NPAIR])
+{
+    const float2 step = make_float2(64.f, 64.f);
+    const float2 dx = q.dx, mf = q.mf, c = q.c, y2 = q.y2, a2 = q.a;
+    constexpr int J0 = Q * (B / 2);
+    if (tier == 1) {
+#pragma unroll
+        for (int j = 0; j < B / 2; ++j) {
+            const float2 x = __ffma2_rn(n2, dx, mf);
+            const float2 m = __ffma2_rn(x, x, c);
+            const float2 d = __ffma2_rn(m, m, y2);
+            float2 r;
+            r.x = rcp_approx(d.x); r.y = rcp_approx(d.y);
+            part[J0 + j] = __ffma2_rn(__ffma2_rn(m, r, r), a2, part[J0 + j]);
+            n2 = __fadd2_rn(n2, step);
+        }
+        return;
+    }
+    const int a = lo16(q.win), b = hi16(q.win);
+    const int c1a = lo16(q.c1), c1b = hi16(q.c1);
+    const int tl = 32 * B * Q + lane;
+    if (tier == 2) {
+        const unsigned wn = (unsigned)(b - a);
+        const unsigned cn = c1b > c1a ? (unsigned)(c1b - c1a) : 0u;
+#pragma unroll
+        for (int j = 0; j < B / 2; ++j) {
+            const float2 x = __ffma2_rn(n2, dx, mf);
+            const float2 m = __ffma2_rn(x, x, c);
+            const float2 d = __ffma2_rn(m, m, y2);
+            float2 r;
+            r.x = rcp_approx(d.x); r.y = rcp_approx(d.y);
+            const float2 v = __fmul2_rn(__ffma2_rn(m, r, r), a2);
+            const int t0 = tl + 64 * j, t1 = t0 + 32;
+            const bool in0 = (unsigned)(t0 - a) < wn && !((unsigned)(t0 - c1a) < cn);
+            const bool in1 = (unsigned)(t1 - a) < wn && !((unsigned)(t1 - c1a) < cn);
+            part[J0 + j].x += in0 ? v.x : 0.f;
+            part[J0 + j].y += in1 ? v.y : 0.f;
+            n2 = __fadd2_rn(n2, step);
+        }
+        return;
+    }
+    /* wide: |x| may exceed 1e8 */
+    const float fc = __int_as_float(q.pad), p = c.x + 1.f;
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+        const int t = tl + 32 * k;
+        if (t < a || t >= b || (t >= c1a && t < c1b)) continue;
+        const float x = fabsf(((n2.x + (float)(32 * k)) - fc) * dx.x);
+        const float x2 = x * x;
+        const float num = x2 + p;
+        float& acc = (k & 1) ? part[J0 + (k >> 1)].y : part[J0 + (k >> 1)].x;
+        acc += (x < 1e18f) ? a2.x / (num - 2.f * (x2 / num)) : 0.f;
+    }
+}
+
+template <int B, int CONS>
+__device__ __forceinline__ void voigt_rs_record(const RecV& r, int lane, float2 lw2,
+                                                float2 (&part)[B * CONS / 2])
+{
+    constexpr int kAll = 0x55555555 & ((1 << (2 * CONS)) - 1);
+    static_assert(CONS == 4, "record-split form: four quarters");
+    const int tiers = r.tiers;
+    const float2 n0 = __fadd2_rn(r.nb, lw2);
+    if (tiers == kAll) {
+        const float2 step = make_float2(64.f, 64.f);
+        const float2 dx = r.dx, mf = r.mf, c = r.c, y2 = r.y2, a2 = r.a;
+        float2 n2 = n0;
+#pragma unroll
+        for (int j = 0; j < B * CONS / 2; ++j) {
+            const float2 x = __ffma2_rn(n2, dx, mf);
+            const float2 m = __ffma2_rn(x, x, c);
+            const float2 d = __ffma2_rn(m, m, y2);
+            float2 rr;
+            rr.x = rcp_approx(d.x); rr.y = rcp_approx(d.y);
+            part[j] = __ffma2_rn(__ffma2_rn(m, rr, rr), a2, part[j]);
+            n2 = __fadd2_rn(n2, step);
+        }
+        return;
+    }
+    /* quarter q starts 32*B*q bins (B/2 pairs of 64) further: exact in float */
+    const float2 qs = make_float2(32.f * B, 32.f * B);
+    const int t0 = tiers & 3, t1 = (tiers >> 2) & 3, t2 = (tiers >> 4) & 3, t3 = (tiers >> 6) & 3;
+    if (t0) voigt_quarter<B, 0>(r, t0, lane, n0, part);
+    if (t1) voigt_quarter<B, 1>(r, t1, lane, __fadd2_rn(n0, qs), part);
+    if (t2) voigt_quarter<B, 2>(r, t2, lane, __ffma2_rn(qs, make_float2(2.f, 2.f), n0), part);
+    if (t3) voigt_quarter<B, 3>(r, t3, lane, __ffma2_rn(qs, make_float2(3.f, 3.f), n0), part);
+}
+
 template <int B>
 __device__ __forceinline__ void lines_voigt_f32(const RecV* __restrict__ rec, int nrec, int warp,
                                                 int lane, float2 (&part)[B / 2])
@@ -1016,10 +1113,23 @@ tile_kernel(const KArgs args)
  * warp has read the stage).  Every wait is bounded: on timeout the thread
  * sets bit GEXS_KERR_PIPELINE of the launch's error word and returns, so a
  * fault in the hand-over ends the kernel with an error instead of a hang.
- * Consumers keep their bins' FP32 partial sums in registers and their
- * Kahan pairs in shared memory (lane-private), so a tile boundary needs no
- * barrier either: the first stage of a tile zeroes them, the last writes
- * the bins out.  Each bin still sums its lines in ascending order. */
+ * Two consumer forms:
+ *  - bins-split (every shape but B = 4 with four consumer warps): warp w
+ *    owns bins [32 B w, 32 B (w+1)) and reads every record; its FP32
+ *    partial sums live in registers and its Kahan pairs in shared memory
+ *    (lane-private), so a tile boundary needs no barrier: the first stage
+ *    of a tile zeroes them, the last writes the bins out.  Each bin sums
+ *    its lines in ascending order.
+ *  - record-split (B = 4, four consumer warps, the default 512-bin tile):
+ *    every warp covers the whole tile (16 bins per lane) and takes every
+ *    fourth record of a stage into Kahan pairs of its own; at the end of a
+ *    tile the warps meet (bounded mbarrier) and each writes a quarter of
+ *    the bins as the sum of the four warps' pairs in warp order.  A record
+ *    is read from shared memory once instead of four times and gives eight
+ *    independent bin-pair chains; measured 200.6 ms against 236.6 ms per
+ *    1e8-line cross-section for the bins-split form of the same shape.
+ * Either way a bin's sum depends only on its tile's records, so results
+ * are bitwise independent of batching. */
 constexpr int WS_STAGES = 4;
 constexpr int WS_R = 128;
 constexpr int WS_SPIN = 1 << 21;          /* default try_wait attempts before giving up */
@@ -1079,7 +1189,10 @@ struct WsSmem {
     static constexpr size_t off_stg = off_bar + (size_t)(2 * WS_STAGES + 2) * sizeof(unsigned long long);
     static constexpr size_t off_gn = off_stg + (size_t)NF64 * 2 * NP * sizeof(double);
     static constexpr size_t off_kahan = (off_gn + (PREP ? 0 : (size_t)2 * NP * sizeof(int)) + 15) & ~size_t(15);
-    static constexpr size_t bytes = off_kahan + (size_t)2 * W * sizeof(float);
+    /* record-split consumers (B = 4, four consumer warps): one Kahan pair
+     * per bin and warp */
+    static constexpr bool RS = (B == 4 && CONS == 4);
+    static constexpr size_t bytes = off_kahan + (size_t)(RS ? CONS : 1) * 2 * W * sizeof(float);
 };
 
 template <int B, int CONS, int PROD, bool PREP>
@@ -1272,78 +1385,170 @@ voigt_ws_kernel(const KArgs args)
         cph ^= 1;
         return ok;
     };
-    float2 part[B / 2];
+    if constexpr (L::RS) {
+        /* record-split: warp w adds records w, w + CONS, ... of every stage
+         * into its own Kahan pairs of all W bins; at the end of a tile the
+         * warps meet, and warp w writes bins [32 B w, 32 B (w+1)) as the sum
+         * of the CONS warps' pairs in warp order */
+        constexpr int BL = B * CONS;
+        float* my_ks = s_ks + (size_t)warp * 2 * W;
+        float* my_kc = my_ks + W;
+        float2 part[BL / 2];
 #pragma unroll
-    for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
-    for (;;) {
-        if (!mbar_wait(s_full + st, ph, args.spin)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
-        const StageHdr h = s_hdr[st];
-        if (h.flags & 4) return;
-        if (h.flags & 1) {
+        for (int j = 0; j < BL / 2; ++j) part[j] = make_float2(0.f, 0.f);
+        const float2 lw2 = make_float2((float)lane, (float)lane);
+        for (;;) {
+            if (!mbar_wait(s_full + st, ph, args.spin)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+            const StageHdr h = s_hdr[st];
+            if (h.flags & 4) return;
+            if (h.flags & 1) {
+#pragma unroll
+                for (int k = 0; k < BL; ++k) { my_ks[lane + 32 * k] = 0.f; my_kc[lane + 32 * k] = 0.f; }
+            }
+            const RecV* rec = s_rec + st * WS_R;
+            for (int i = warp; i < h.nrec; i += CONS) voigt_rs_record<B, CONS>(rec[i], lane, lw2, part);
+#pragma unroll
+            for (int k = 0; k < BL; ++k) {
+                const int t = lane + 32 * k;
+                float ks = my_ks[t], kc = my_kc[t];
+                kahan_add(ks, kc, (k & 1) ? part[k >> 1].y : part[k >> 1].x);
+                my_ks[t] = ks; my_kc[t] = kc;
+            }
+#pragma unroll
+            for (int j = 0; j < BL / 2; ++j) part[j] = make_float2(0.f, 0.f);
+            /* the stage's records are consumed: hand the slot back first */
+            __syncwarp();
+            if (lane == 0) mbar_arrive(s_empty + st);
+            if (++st == WS_STAGES) { st = 0; ph ^= 1; }
+            if (!(h.flags & 2)) continue;
+            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+            double v[B];
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const int t = warp * 32 * B + lane + 32 * k;
-                s_ks[t] = 0.f; s_kc[t] = 0.f;
+                double acc = 0.0;
+#pragma unroll
+                for (int w = 0; w < CONS; ++w)
+                    acc += (double)s_ks[(size_t)w * 2 * W + t] - (double)s_ks[(size_t)w * 2 * W + W + t];
+                v[k] = acc;
             }
-        }
-        const RecV* rec = s_rec + st * WS_R;
-        lines_voigt_f32<B>(rec, h.nrec, warp, lane, part);
-#pragma unroll
-        for (int k = 0; k < B; ++k) {
-            const int t = warp * 32 * B + lane + 32 * k;
-            float ks = s_ks[t], kc = s_kc[t];
-            kahan_add(ks, kc, bin_acc<B>(part, k));
-            s_ks[t] = ks; s_kc[t] = kc;
-        }
-#pragma unroll
-        for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
-        if ((h.flags & 2) && !(h.flags & 8)) {
             const gexs_job& J = args.jobs[h.jl];
             double* out = J.out;
-#pragma unroll
-            for (int k = 0; k < B; ++k) {
-                const int t = warp * 32 * B + lane + 32 * k;
-                if (t < h.jn) {
-                    const double v = (double)s_ks[t] - (double)s_kc[t];
-                    const int64_t j = h.j0 + t;
-                    out[j] = J.accumulate ? out[j] + v : v;
-                }
-            }
-        } else if (h.flags & 2) {
-            /* one slice of a split tile: its partial row, then a ticket; the
-             * last slice to finish adds the rows in slice order */
-            const gexs_job& J = args.jobs[h.jl];
-            double* out = J.out;
-            const int base = args.sl.prefix[h.tile];
-            const int ns = args.sl.prefix[h.tile + 1] - base;
-            const int rb = args.sl.rowbase[h.tile];
-            double* row = args.sl.rows + (size_t)(rb + (h.item - base)) * W;
-#pragma unroll
-            for (int k = 0; k < B; ++k) {
-                const int t = warp * 32 * B + lane + 32 * k;
-                if (t < h.jn) row[t] = (double)s_ks[t] - (double)s_kc[t];
-            }
-            __threadfence();
-            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
-            if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile, 1) == ns - 1;
-            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
-            if (s_last) {
-                __threadfence();
+            if (!(h.flags & 8)) {
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
                     const int t = warp * 32 * B + lane + 32 * k;
                     if (t < h.jn) {
-                        double v = 0.0;
-                        for (int q = 0; q < ns; ++q) v += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
+                        const int64_t j = h.j0 + t;
+                        out[j] = J.accumulate ? out[j] + v[k] : v[k];
+                    }
+                }
+            } else {
+                const int base = args.sl.prefix[h.tile];
+                const int ns = args.sl.prefix[h.tile + 1] - base;
+                const int rb = args.sl.rowbase[h.tile];
+                double* row = args.sl.rows + (size_t)(rb + (h.item - base)) * W;
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    if (t < h.jn) row[t] = v[k];
+                }
+                __threadfence();
+                if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+                if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile, 1) == ns - 1;
+                if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+                if (s_last) {
+                    __threadfence();
+#pragma unroll
+                    for (int k = 0; k < B; ++k) {
+                        const int t = warp * 32 * B + lane + 32 * k;
+                        if (t < h.jn) {
+                            double acc = 0.0;
+                            for (int q = 0; q < ns; ++q) acc += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
+                            const int64_t j = h.j0 + t;
+                            out[j] = J.accumulate ? out[j] + acc : acc;
+                        }
+                    }
+                }
+            }
+            /* every warp has read the Kahan pairs before the next tile clears them */
+            if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+        }
+    }
+    else {
+        float2 part[B / 2];
+#pragma unroll
+        for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
+        for (;;) {
+            if (!mbar_wait(s_full + st, ph, args.spin)) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+            const StageHdr h = s_hdr[st];
+            if (h.flags & 4) return;
+            if (h.flags & 1) {
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    s_ks[t] = 0.f; s_kc[t] = 0.f;
+                }
+            }
+            const RecV* rec = s_rec + st * WS_R;
+            lines_voigt_f32<B>(rec, h.nrec, warp, lane, part);
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const int t = warp * 32 * B + lane + 32 * k;
+                float ks = s_ks[t], kc = s_kc[t];
+                kahan_add(ks, kc, bin_acc<B>(part, k));
+                s_ks[t] = ks; s_kc[t] = kc;
+            }
+#pragma unroll
+            for (int j = 0; j < B / 2; ++j) part[j] = make_float2(0.f, 0.f);
+            if ((h.flags & 2) && !(h.flags & 8)) {
+                const gexs_job& J = args.jobs[h.jl];
+                double* out = J.out;
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    if (t < h.jn) {
+                        const double v = (double)s_ks[t] - (double)s_kc[t];
                         const int64_t j = h.j0 + t;
                         out[j] = J.accumulate ? out[j] + v : v;
                     }
                 }
+            } else if (h.flags & 2) {
+                /* one slice of a split tile: its partial row, then a ticket; the
+                 * last slice to finish adds the rows in slice order */
+                const gexs_job& J = args.jobs[h.jl];
+                double* out = J.out;
+                const int base = args.sl.prefix[h.tile];
+                const int ns = args.sl.prefix[h.tile + 1] - base;
+                const int rb = args.sl.rowbase[h.tile];
+                double* row = args.sl.rows + (size_t)(rb + (h.item - base)) * W;
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = warp * 32 * B + lane + 32 * k;
+                    if (t < h.jn) row[t] = (double)s_ks[t] - (double)s_kc[t];
+                }
+                __threadfence();
+                if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+                if (tid == 0) s_last = atomicAdd(args.sl.ticket + h.tile, 1) == ns - 1;
+                if (!csync()) { atomicOr(args.err, GEXS_KERR_PIPELINE); return; }
+                if (s_last) {
+                    __threadfence();
+#pragma unroll
+                    for (int k = 0; k < B; ++k) {
+                        const int t = warp * 32 * B + lane + 32 * k;
+                        if (t < h.jn) {
+                            double v = 0.0;
+                            for (int q = 0; q < ns; ++q) v += __ldcg(args.sl.rows + (size_t)(rb + q) * W + t);
+                            const int64_t j = h.j0 + t;
+                            out[j] = J.accumulate ? out[j] + v : v;
+                        }
+                    }
+                }
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(s_empty + st);
+            if (++st == WS_STAGES) { st = 0; ph ^= 1; }
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(s_empty + st);
-        if (++st == WS_STAGES) { st = 0; ph ^= 1; }
     }
 }
 

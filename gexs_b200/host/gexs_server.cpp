@@ -8,10 +8,12 @@
  *      grids fit in the HBM budget and the in-flight cap allows;
  *   3. the admitted group gets Q(T) from the resident table of its list
  *      (or the partition kernel on the worker's own stream for temperatures
- *      outside it), stream-ordered output buffers from the server's own
- *      memory pool (cudaMallocFromPoolAsync; freed pages stay mapped) and
- *      one gexs_run launch on the next stream of the server, followed by an
- *      event.
+ *      outside it), stream-ordered output buffers from the context's
+ *      memory pool, which also holds the launch's scratch and keeps freed
+ *      pages mapped, and one gexs_run launch on the next stream of the
+ *      server, followed by an event.  A request is admitted for its output
+ *      and the scratch its job takes (prep arrays, tables, slice rows), so
+ *      what the pool holds stays within the budget.
  * Nothing on this path synchronises the device (no cudaMalloc/cudaFree),
  * so a new batch starts while earlier ones still run.  A request's output
  * is released when the caller fetches it (gexs_server_wait), which frees
@@ -123,10 +125,6 @@ struct gexs_server {
     int* d_errs = nullptr;
     int* h_errs = nullptr;
     std::vector<int> free_slots;
-    /* request outputs: a pool of the server's own that keeps freed memory
-     * mapped (admission bounds what it holds), so a request never waits
-     * for pages the previous one gave back */
-    cudaMemPool_t out_pool = nullptr;
 
     /* a deque: adding a list never moves the others, which the worker
      * reads without the lock while it launches */
@@ -241,7 +239,9 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
             j.lines.nu = L.nu; j.lines.elow = L.elow; j.lines.aif = L.aif; j.lines.gns = L.gns;
             j.lines.gamma = L.gamma; j.lines.n = L.n; j.lines.count = L.count;
             void* d = nullptr;
-            if (cudaMallocFromPoolAsync(&d, r->bytes, s->out_pool, st) != cudaSuccess) {
+            cudaMemPool_t pool = gexs::ctx_pool(s->ctx);
+            if ((pool ? cudaMallocFromPoolAsync(&d, output_bytes(r->r), pool, st)
+                      : cudaMallocAsync(&d, output_bytes(r->r), st)) != cudaSuccess) {
                 status = GEXS_ERR_OOM;
                 break;
             }
@@ -410,19 +410,6 @@ int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int stre
               cudaMallocHost(&s->h_errs, sizeof(int) * s->max_inflight) == cudaSuccess;
     for (int i = s->max_inflight - 1; ok && i >= 0; --i) s->free_slots.push_back(i);
     if (!ok) { gexs_server_destroy(s); return gexs::set_error(GEXS_ERR_OOM, "server buffers"); }
-    {
-        cudaMemPoolProps props;
-        std::memset(&props, 0, sizeof(props));
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = device;
-        uint64_t keep = UINT64_MAX;
-        if (cudaMemPoolCreate(&s->out_pool, &props) != cudaSuccess ||
-            cudaMemPoolSetAttribute(s->out_pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
-            gexs_server_destroy(s);
-            return gexs::set_error(GEXS_ERR_CUDA, "server output pool");
-        }
-    }
     s->worker = std::thread(worker_loop, s);
     *out = s;
     return GEXS_OK;
@@ -456,7 +443,6 @@ int gexs_server_destroy(gexs_server* s)
     cudaFree(s->d_betas); cudaFree(s->d_partial); cudaFree(s->d_q);
     cudaFree(s->d_errs);
     if (s->h_errs) cudaFreeHost(s->h_errs);
-    if (s->out_pool) cudaMemPoolDestroy(s->out_pool);
     gexs_ctx_destroy(s->ctx);
     delete s;
     return GEXS_OK;
@@ -550,24 +536,41 @@ int gexs_server_submit(gexs_server* s, const gexs_request* r, uint64_t* ticket)
     q->r = *r;
     if (!(q->r.ref_temp > 0)) q->r.ref_temp = 296.0;
     if (q->r.profile != GEXS_VOIGT_QUAD) q->r.quad_nodes = 16;
-    q->bytes = output_bytes(*r);
     std::memset(&q->info, 0, sizeof(q->info));
     q->info.evals = -1;
     {
-        std::lock_guard<std::mutex> g(s->mu);
-        if (r->list_id < 0 || r->list_id >= (int)s->lists.size()) {
-            delete q;
-            return gexs::set_error(GEXS_ERR_INVALID, "unknown list_id");
+        /* admission counts the output and the scratch of the job's launch
+         * (prep arrays, tables, slice rows), all from the context's pool */
+        {
+            std::lock_guard<std::mutex> g(s->mu);
+            if (r->list_id < 0 || r->list_id >= (int)s->lists.size()) {
+                delete q;
+                return gexs::set_error(GEXS_ERR_INVALID, "unknown list_id");
+            }
+            const List& L = s->lists[r->list_id];
+            probe.lines.nu = L.nu; probe.lines.elow = L.elow; probe.lines.aif = L.aif;
+            probe.lines.gns = L.gns; probe.lines.gamma = L.gamma; probe.lines.n = L.n;
+            probe.lines.count = L.count;
         }
-        const List& L = s->lists[r->list_id];
         bool press = r->profile == GEXS_VOIGT || r->profile == GEXS_VOIGT_QUAD;
-        if (press && !L.gamma) {
+        if (press && !probe.lines.gamma) {
             delete q;
             return gexs::set_error(GEXS_ERR_INVALID, "list has no broadening for this profile");
         }
+        probe.precision = q->r.precision;
+        probe.quad_nodes = q->r.quad_nodes;
+        double placeholder = 0.0;          /* never written: sizes only */
+        probe.out = &placeholder;
+        size_t scratch = 0;
+        st = gexs::run_scratch_bytes(s->ctx, &probe, 1, nullptr, &scratch);
+        if (st) { delete q; return st; }
+        q->bytes = output_bytes(*r) + scratch;
+    }
+    {
+        std::lock_guard<std::mutex> g(s->mu);
         if (s->resident + q->bytes > s->budget) {
             delete q;
-            return gexs::set_error(GEXS_ERR_ADMISSION, "request output exceeds the HBM budget");
+            return gexs::set_error(GEXS_ERR_ADMISSION, "request output and scratch exceed the HBM budget");
         }
         if (s->stop) { delete q; return gexs::set_error(GEXS_ERR_SHUTDOWN, "server stopping"); }
         q->id = s->next_id++;
@@ -617,7 +620,7 @@ int gexs_server_wait(gexs_server* s, uint64_t ticket, int timeout_ms, double* h_
         cudaError_t e = cudaSuccess;
         if (r->done) e = cudaStreamWaitEvent(c, r->done, 0);
         if (e == cudaSuccess && h_out && !status)
-            e = cudaMemcpyAsync(h_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, c);
+            e = cudaMemcpyAsync(h_out, r->d_out, output_bytes(r->r), cudaMemcpyDeviceToHost, c);
         cudaError_t e2 = cudaFreeAsync(r->d_out, c);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaStreamSynchronize(c);

@@ -112,7 +112,9 @@ def test_served_results_match_oracle(served, small_states, small_lines):
 def test_admission_by_budget(small_states, small_lines):
     line_bytes = sum(v.nbytes for v in small_lines.values()) + small_states.energy.nbytes * 2
     G = 200000
-    budget = line_bytes + 3 * G * 8 + 4096      # room for three outputs at a time
+    # room for about three outputs; a request is also charged the scratch of
+    # its launch (prep arrays, tables, slice rows), so two run at a time
+    budget = line_bytes + 3 * G * 8 + 4096
     srv = Server(0, hbm_budget=budget, streams=2)
     try:
         lid = srv.add_list(small_lines, small_states.energy, small_states.g, 18.0)
