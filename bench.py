@@ -598,9 +598,11 @@ def serve_bench(torch, dev, local_rank, args):
         for th in threads:
             th.join()
         wall = time.perf_counter() - t0
-        if errors:
+        if len(errors) == n:
             raise RuntimeError(errors[0])
-        return wall, np.array(lat), np.array(dlat), infos
+        ok = [i for i in range(n) if infos[i] is not None]
+        return (wall, np.array([lat[i] for i in ok]), np.array([dlat[i] for i in ok]),
+                [infos[i] for i in ok], errors)
 
     log("serving: %d requests, serial pass" % len(reqs))
     # warm-up (module loads, pools), then the set one request at a time
@@ -614,14 +616,16 @@ def serve_bench(torch, dev, local_rank, args):
     for k, load in enumerate(args.serve_loads):
         rate = load / service
         log("serving: offered load %.2f" % load)
-        wall, lat, dlat, infos = run(rate, 4100 + k)
+        wall, lat, dlat, infos, errors = run(rate, 4100 + k)
         rates.append({"offered_load": load, "offered_req_per_s": rate, "requests": len(reqs),
+                      "failed": len(errors), "first_error": errors[0] if errors else None,
                       "p50_ms": float(np.percentile(lat, 50)),
                       "p99_ms": float(np.percentile(lat, 99)),
                       "mean_ms": float(lat.mean()),
                       "device_done_p50_ms": float(np.percentile(dlat, 50)),
                       "device_done_p99_ms": float(np.percentile(dlat, 99)),
-                      "throughput_req_per_s": len(reqs) / wall, "evals_per_s": ev / wall,
+                      "throughput_req_per_s": len(infos) / wall,
+                      "evals_per_s": ev / wall if not errors else None,
                       "mean_batch": float(np.mean([i.batch_size for i in infos])),
                       "max_batch": int(max(i.batch_size for i in infos))})
     stats = srv.stats()

@@ -86,6 +86,20 @@ namespace gexs {
 int ctx_device(gexs_ctx* c) { return c->device; }
 int ctx_sm_count(gexs_ctx* c) { return c->nsm; }
 cudaMemPool_t ctx_pool(gexs_ctx* c) { return c->pool; }
+
+cudaError_t pool_alloc(cudaMemPool_t pool, void** p, size_t bytes, cudaStream_t s)
+{
+    if (!pool) return cudaMallocAsync(p, bytes, s);
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
+    if (e == cudaErrorMemoryAllocation) {
+        /* the pool keeps freed pages mapped; when they are too fragmented
+         * for this size, give back what no allocation uses and retry once */
+        cudaGetLastError();
+        cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocFromPoolAsync(p, bytes, pool, s);
+    }
+    return e;
+}
 }  // namespace gexs
 
 static gexs_launch_cfg default_cfg(int pk, int prec)
@@ -492,8 +506,7 @@ int gexs::run_jobs(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs_la
         if (!prep && has_compact(g)) return set_error(GEXS_ERR_INVALID, "compact line lists need the prep arrays");
         Layout L = group_layout(g, prep, cfgs[gi]);
         void* d = nullptr;
-        e = ctx->pool ? cudaMallocFromPoolAsync(&d, L.bytes, ctx->pool, s)
-                      : cudaMallocAsync(&d, L.bytes, s);
+        e = pool_alloc(ctx->pool, &d, L.bytes, s);
         if (e != cudaSuccess) return set_error(GEXS_ERR_OOM, "launch tables");
         /* the image carries the zeroed work counters */
         std::vector<unsigned char> h = group_image(g, L, (unsigned char*)d, prep);

@@ -86,6 +86,9 @@ int run_scratch_bytes(gexs_ctx* ctx, const gexs_job* jobs, int njobs, const gexs
 int ctx_device(gexs_ctx* c);
 int ctx_sm_count(gexs_ctx* c);
 cudaMemPool_t ctx_pool(gexs_ctx* c);
+/* stream-ordered allocation from a pool (NULL: the device default); on an
+ * out-of-memory the pool's unused pages are released and the call retried */
+cudaError_t pool_alloc(cudaMemPool_t pool, void** p, size_t bytes, cudaStream_t s);
 
 /* error reporting (gexs_capi.cu): thread-local message, returns status */
 int set_error(int status, const std::string& msg);

@@ -152,6 +152,10 @@ struct gexs_server {
     std::vector<cudaStream_t> copy_free;
 
     int64_t n_submitted = 0, n_completed = 0, n_batches = 0;
+    /* a group that could not get its memory while other batches ran went
+     * back to the queue; admission waits for one of those to complete */
+    bool oom_hold = false;
+    int64_t oom_mark = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
     double now_ms() const
@@ -239,9 +243,7 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
             j.lines.nu = L.nu; j.lines.elow = L.elow; j.lines.aif = L.aif; j.lines.gns = L.gns;
             j.lines.gamma = L.gamma; j.lines.n = L.n; j.lines.count = L.count;
             void* d = nullptr;
-            cudaMemPool_t pool = gexs::ctx_pool(s->ctx);
-            if ((pool ? cudaMallocFromPoolAsync(&d, output_bytes(r->r), pool, st)
-                      : cudaMallocAsync(&d, output_bytes(r->r), st)) != cudaSuccess) {
+            if (gexs::pool_alloc(gexs::ctx_pool(s->ctx), &d, output_bytes(r->r), st) != cudaSuccess) {
                 status = GEXS_ERR_OOM;
                 break;
             }
@@ -271,6 +273,27 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
         status = GEXS_ERR_CUDA;
     if (!status && cudaEventRecord(b.ev, st) != cudaSuccess) status = GEXS_ERR_CUDA;
     std::lock_guard<std::mutex> g(s->mu);
+    if (status == GEXS_ERR_OOM && !s->running.empty()) {
+        /* out of memory while earlier batches still hold theirs (the pool's
+         * pages can be too fragmented for a large prep array): undo the
+         * admission, put the group back at the head of the queue in arrival
+         * order and admit again after the next completion */
+        cudaStreamSynchronize(st);
+        if (b.ev) cudaEventDestroy(b.ev);
+        if (b.slot >= 0) s->free_slots.push_back(b.slot);
+        for (auto it = adm.rbegin(); it != adm.rend(); ++it) {
+            Req* r = *it;
+            if (r->d_out) { cudaFreeAsync(r->d_out, st); r->d_out = nullptr; }
+            r->state = RQ_PENDING;
+            s->inflight--;
+            s->inflight_bytes -= r->bytes;
+            s->pending.push_front(r);
+        }
+        cudaGetLastError();
+        s->oom_hold = true;
+        s->oom_mark = s->n_completed;
+        return;
+    }
     s->n_batches++;
     for (Req* r : adm) {
         r->info.batch_size = (int)adm.size();
@@ -335,7 +358,8 @@ void worker_loop(gexs_server* s)
         /* 2. admission in arrival order */
         const size_t cap = s->budget > s->resident ? s->budget - s->resident : 0;
         std::vector<Req*> adm;
-        while (!s->pending.empty()) {
+        if (s->oom_hold && (s->n_completed != s->oom_mark || s->running.empty())) s->oom_hold = false;
+        while (!s->oom_hold && !s->pending.empty()) {
             Req* r = s->pending.front();
             if (s->inflight >= s->max_inflight || s->inflight_bytes + r->bytes > cap) break;
             s->pending.pop_front();

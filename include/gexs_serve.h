@@ -4,7 +4,7 @@
  * No counterpart in the reference, which computes one configured run per
  * process (main.cpp:17-42).  The server keeps line lists, their states and
  * a Q(T) table per list resident in HBM, admits requests while their output
- * grids fit in the memory budget, and launches every group of newly
+ * grids and launch scratch fit in the memory budget, and launches every group of newly
  * admitted requests as one persistent launch on one of several streams, so
  * requests that arrive while others run overlap with them on the device
  * (continuous batching).  The Q(T) table holds the device sum over the
@@ -61,13 +61,14 @@ typedef struct gexs_request_info {
 } gexs_request_info;
 
 /* device: CUDA device; hbm_budget: bytes the server may use for resident
- * lists plus in-flight outputs (0 = 90% of free memory); max_inflight:
- * admitted-but-unfetched requests at most (0 = 256); streams: launch
- * streams (0 = 4).  Each launch's scratch is not part of the budget: it
- * comes from the context's memory pool, 24 B per line of prep arrays plus
- * the line-slice tables (at most 1 GiB of partial rows for region I and
- * 1 GiB for the Voigt core), so leave that much outside the budget per
- * stream. */
+ * lists plus in-flight requests (0 = 90% of the memory free when it is
+ * created: memory the caller allocates afterwards is not seen, so pass a
+ * budget then); max_inflight: admitted-but-unfetched requests at most
+ * (0 = 256); streams: launch streams (0 = 4).  A request is charged its
+ * output grid plus the scratch its launch takes from the context's memory
+ * pool (launch tables, 24 B per line of prep arrays, line-slice rows), held
+ * until the result is fetched; outputs come from the same pool, which keeps
+ * freed pages mapped, so what the server holds stays within the budget. */
 int gexs_server_create(int device, size_t hbm_budget, int max_inflight, int streams,
                        gexs_server** out);
 int gexs_server_destroy(gexs_server* s);
