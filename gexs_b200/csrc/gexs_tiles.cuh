@@ -725,12 +725,29 @@ __device__ __forceinline__ void voigt_quarter(const RecV& q, int tier, int lane,
     }
 }
 
+/* quarters Q .. CONS-1 of a record that is not full everywhere */
+template <int B, int Q, int CONS>
+struct RsQuarters {
+    static __device__ __forceinline__ void run(const RecV& r, int tiers, int lane, float2 n0,
+                                               float2 (&part)[B * CONS / 2])
+    {
+        const int t = (tiers >> (2 * Q)) & 3;
+        /* quarter Q starts 32 B Q bins further: exact in float */
+        if (t) voigt_quarter<B, Q>(r, t, lane, __fadd2_rn(n0, make_float2(32.f * B * Q, 32.f * B * Q)),
+                                   part);
+        RsQuarters<B, Q + 1, CONS>::run(r, tiers, lane, n0, part);
+    }
+};
+template <int B, int CONS>
+struct RsQuarters<B, CONS, CONS> {
+    static __device__ __forceinline__ void run(const RecV&, int, int, float2, float2 (&)[B * CONS / 2]) {}
+};
+
 template <int B, int CONS>
 __device__ __forceinline__ void voigt_rs_record(const RecV& r, int lane, float2 lw2,
                                                 float2 (&part)[B * CONS / 2])
 {
     constexpr int kAll = 0x55555555 & ((1 << (2 * CONS)) - 1);
-    static_assert(CONS == 4, "record-split form: four quarters");
     const int tiers = r.tiers;
     const float2 n0 = __fadd2_rn(r.nb, lw2);
     if (tiers == kAll) {
@@ -749,13 +766,7 @@ __device__ __forceinline__ void voigt_rs_record(const RecV& r, int lane, float2 
         }
         return;
     }
-    /* quarter q starts 32*B*q bins (B/2 pairs of 64) further: exact in float */
-    const float2 qs = make_float2(32.f * B, 32.f * B);
-    const int t0 = tiers & 3, t1 = (tiers >> 2) & 3, t2 = (tiers >> 4) & 3, t3 = (tiers >> 6) & 3;
-    if (t0) voigt_quarter<B, 0>(r, t0, lane, n0, part);
-    if (t1) voigt_quarter<B, 1>(r, t1, lane, __fadd2_rn(n0, qs), part);
-    if (t2) voigt_quarter<B, 2>(r, t2, lane, __ffma2_rn(qs, make_float2(2.f, 2.f), n0), part);
-    if (t3) voigt_quarter<B, 3>(r, t3, lane, __ffma2_rn(qs, make_float2(3.f, 3.f), n0), part);
+    RsQuarters<B, 0, CONS>::run(r, tiers, lane, n0, part);
 }
 
 template <int B>
@@ -1114,20 +1125,21 @@ tile_kernel(const KArgs args)
  * sets bit GEXS_KERR_PIPELINE of the launch's error word and returns, so a
  * fault in the hand-over ends the kernel with an error instead of a hang.
  * Two consumer forms:
- *  - bins-split (every shape but B = 4 with four consumer warps): warp w
+ *  - bins-split (every shape but the 512-bin tiles): warp w
  *    owns bins [32 B w, 32 B (w+1)) and reads every record; its FP32
  *    partial sums live in registers and its Kahan pairs in shared memory
  *    (lane-private), so a tile boundary needs no barrier: the first stage
  *    of a tile zeroes them, the last writes the bins out.  Each bin sums
  *    its lines in ascending order.
- *  - record-split (B = 4, four consumer warps, the default 512-bin tile):
- *    every warp covers the whole tile (16 bins per lane) and takes every
- *    fourth record of a stage into Kahan pairs of its own; at the end of a
- *    tile the warps meet (bounded mbarrier) and each writes a quarter of
- *    the bins as the sum of the four warps' pairs in warp order.  A record
- *    is read from shared memory once instead of four times and gives eight
- *    independent bin-pair chains; measured 200.6 ms against 236.6 ms per
- *    1e8-line cross-section for the bins-split form of the same shape.
+ *  - record-split (512-bin tiles: B = 4 with four consumer warps, the
+ *    default, or B = 2 with eight): every warp covers the whole tile (16
+ *    bins per lane) and takes every CONS-th record of a stage into Kahan
+ *    pairs of its own; at the end of a tile the warps meet (bounded
+ *    mbarrier) and warp w writes its 32 B bins as the sum of all warps'
+ *    pairs in warp order.  A record is read from shared memory once instead
+ *    of CONS times and gives eight independent bin-pair chains; measured
+ *    200.6 ms against 236.6 ms per 1e8-line cross-section for the
+ *    bins-split form of the 4 x 4 shape (229 against 348 ms for 2 x 8).
  * Either way a bin's sum depends only on its tile's records, so results
  * are bitwise independent of batching. */
 constexpr int WS_STAGES = 4;
@@ -1189,9 +1201,9 @@ struct WsSmem {
     static constexpr size_t off_stg = off_bar + (size_t)(2 * WS_STAGES + 2) * sizeof(unsigned long long);
     static constexpr size_t off_gn = off_stg + (size_t)NF64 * 2 * NP * sizeof(double);
     static constexpr size_t off_kahan = (off_gn + (PREP ? 0 : (size_t)2 * NP * sizeof(int)) + 15) & ~size_t(15);
-    /* record-split consumers (B = 4, four consumer warps): one Kahan pair
-     * per bin and warp */
-    static constexpr bool RS = (B == 4 && CONS == 4);
+    /* record-split consumers (512-bin tiles: B = 4 with four consumer
+     * warps, B = 2 with eight): one Kahan pair per bin and warp */
+    static constexpr bool RS = (B * CONS == 16);
     static constexpr size_t bytes = off_kahan + (size_t)(RS ? CONS : 1) * 2 * W * sizeof(float);
 };
 
