@@ -141,6 +141,35 @@ __device__ __forceinline__ R hum_region4(R x, R y)
     return expcos(ur, ui) - re_div(nr, ni, qr, qi);
 }
 
+/* Region IV for the FP32 form's core kernel: the rational part in FP64
+ * (its real part comes out of a mostly imaginary quotient, so FP32 rounding
+ * would be amplified), exp(U) cos(Im U) in FP32.  In region IV |x| < 5.5 and
+ * y < 0.195|x| - 0.176, so Re U >= -30.25 (no underflow), |Im U| < 10, and
+ * Re w = exp-term + a non-negative part: the FP32 error of the exp term
+ * (a few 1e-7 of that term) is at most a few 1e-7 of the result. */
+__device__ __forceinline__ double hum_region4_core(double x, double y)
+{
+    const double ur = y * y - x * x, ui = -2.0 * x * y;
+    const double vr = -ur, vi = -ui;
+    double pr = .56419, pi = 0.0;
+    cmul_add(pr, pi, vr, vi, 1.320522);
+    cmul_add(pr, pi, vr, vi, 35.76683);
+    cmul_add(pr, pi, vr, vi, 219.0313);
+    cmul_add(pr, pi, vr, vi, 1540.787);
+    cmul_add(pr, pi, vr, vi, 3321.9905);
+    cmul_add(pr, pi, vr, vi, 36183.31);
+    double qr = 1.0, qi = 0.0;
+    cmul_add(qr, qi, vr, vi, 1.841439);
+    cmul_add(qr, qi, vr, vi, 61.57037);
+    cmul_add(qr, qi, vr, vi, 364.2191);
+    cmul_add(qr, qi, vr, vi, 2186.181);
+    cmul_add(qr, qi, vr, vi, 9022.228);
+    cmul_add(qr, qi, vr, vi, 24322.84);
+    cmul_add(qr, qi, vr, vi, 32066.6);
+    const double nr = y * pr + x * pi, ni = y * pi - x * pr;
+    return (double)expcos<float>((float)ur, (float)ui) - re_div(nr, ni, qr, qi);
+}
+
 /* region selected by integer bin limits: 1..4 */
 template <typename R>
 __device__ __forceinline__ R hum_by_region(int reg, R x, R y)

@@ -1577,8 +1577,9 @@ voigt_ws_kernel(const KArgs args)
  * per lane, derived in FP64 with the region-I kernel's predicates.  A warp
  * then steps through the union of its 32 lines' cores bin by bin: at bin t
  * every lane evaluates its own line in the region t falls in (II in FP32,
- * III and IV in FP64), a butterfly of shuffles sums the 32 terms in a fixed
- * order, and lane 0 adds the sum into the warp's row of doubles.  Lines that
+ * III and the rational part of IV in FP64, IV's exp term in FP32), a
+ * butterfly of shuffles sums the 32 terms in a fixed order, and lane 0
+ * adds the sum into the warp's row of doubles.  Lines that
  * are neighbours in nu have overlapping cores, so most lanes work at every
  * step and no lane scans for work.  A bin receives its core terms in a
  * fixed order (groups of 32 lines in ascending order per warp, rows added
@@ -1724,7 +1725,7 @@ core_kernel(const KArgs args)
                         } else {
                             const double x = dmul(fabs(dsub(grid_f(J.nu_start, J.dnu, T.j0 + t), nu)), invw);
                             v = amp * ((t >= c3a && t < c3b) ? hum_region3<double>(x, y)
-                                                             : hum_region4<double>(x, y));
+                                                             : hum_region4_core(x, y));
                         }
                     }
                     /* fixed-order sum of the 32 lines' terms; lane 0's value is used */
