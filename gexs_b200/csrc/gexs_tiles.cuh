@@ -1716,7 +1716,7 @@ core_kernel(const KArgs args)
                     ulo = min(ulo, __shfl_xor_sync(0xffffffffu, ulo, o));
                     uhi = max(uhi, __shfl_xor_sync(0xffffffffu, uhi, o));
                 }
-                for (int t = ulo; t < uhi; ++t) {
+                auto term = [&](int t) -> double {
                     double v = 0.0;
                     if (has && t >= c1a && t < c1b) {
                         if (t < c2a || t >= c2b) {
@@ -1728,10 +1728,24 @@ core_kernel(const KArgs args)
                                                              : hum_region4_core(x, y));
                         }
                     }
-                    /* fixed-order sum of the 32 lines' terms; lane 0's value is used */
+                    return v;
+                };
+                /* two bins per step: their butterflies are independent, so the
+                 * shuffles of one overlap the other's; each bin's terms are
+                 * summed in the same order as one bin per step */
+                for (int t = ulo; t < uhi; t += 2) {
+                    const bool two = t + 1 < uhi;      /* warp-uniform */
+                    double v0 = term(t);
+                    double v1 = two ? term(t + 1) : 0.0;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0) row[t] += v;
+                    for (int o = 16; o > 0; o >>= 1) {
+                        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+                        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+                    }
+                    if (lane == 0) {
+                        row[t] += v0;
+                        if (two) row[t + 1] += v1;
+                    }
                 }
             }
             __syncthreads();
