@@ -511,7 +511,8 @@ def serve_bench(torch, dev, local_rank, args):
 
     Three resident synthetic lists of 1e7, 1e8 and 5e8 lines times
     --serve-scale (18, 16, 44 amu; generated as the 1e8-line workload, the
-    largest from 1e6 states J 0-120).  One seeded set of --serve-requests
+    largest from 1e6 states J 0-120), kept in the compact layout (FP64 nu0,
+    float E'', g'A, gamma, n: 24 B per line).  One seeded set of --serve-requests
     requests is used for every rate: list uniform, T log-U(100, 3000) K, P
     log-U(1e-6, 100) bar, dnu log-U(0.001, 0.1) cm^-1, 1e4-1e7 points (at
     most the span 100-20000 allows), start uniform in 100-20000 minus the
@@ -536,7 +537,7 @@ def serve_bench(torch, dev, local_rank, args):
         big = k == 3
         st = synth.make_states(1000000 if big else 200000, 120 if big else 80, 1010 + k)
         L = synth.make_lines_torch(st, n, NU0, NU1, 2010 + k, broadening_seed=3010 + k, device=dev)
-        lid = srv.add_list(L, st.energy, st.g, mass)
+        lid = srv.add_list(L, st.energy, st.g, mass, compact=True)
         keep.append(LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev))
         lists.append((lid, mass, n))
         del L
@@ -637,6 +638,8 @@ def serve_bench(torch, dev, local_rank, args):
     stats = srv.stats()
     srv.close()
     return {"lists": [{"lines": n, "mass_amu": m} for _, m, n in lists],
+            "list_layout": "resident compact: FP64 nu0 + float E'', g'A, gamma, n (24 B/line), "
+                           "%.1f GB of lines" % (24.0 * sum(n for _, _, n in lists) / 1e9),
             "list_scale": scale, "list_generation_s": t_gen,
             "serial_service_ms": 1e3 * service, "evals_per_request_set": ev,
             "rates": rates, "batches": stats["batches"],

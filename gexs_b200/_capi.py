@@ -167,6 +167,8 @@ SIGNATURES = [
     ("gexs_server_destroy", C.c_int, [C.c_void_p]),
     ("gexs_server_add_list", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 +
      [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int)]),
+    ("gexs_server_add_lines", C.c_int, [C.c_void_p, C.POINTER(GexsLines), C.c_void_p, C.c_void_p,
+                                        C.c_int64, C.c_double, C.POINTER(C.c_int)]),
     ("gexs_server_submit", C.c_int, [C.c_void_p, C.POINTER(GexsRequest), C.POINTER(C.c_uint64)]),
     ("gexs_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p,
                                    C.POINTER(GexsRequestInfo)]),

@@ -386,13 +386,23 @@ class Server:
             return C.c_void_p(a.data_ptr())
         return a.ctypes.data_as(C.c_void_p)
 
-    def add_list(self, lines, state_energy, state_g, mass):
+    def add_list(self, lines, state_energy, state_g, mass, compact=False):
         """lines: dict of arrays nu, elow, aif, gns[, gamma, n] (numpy host
-        arrays or contiguous torch tensors, host or device)."""
+        arrays or contiguous torch tensors, host or device), or a LineList.
+        compact=True keeps the list resident in the 24-byte layout (FP64 nu,
+        float E'', g'A, gamma, n; gexs_server_add_lines)."""
         lid = C.c_int()
         se = np.ascontiguousarray(state_energy, dtype=np.float64)
         sg = np.ascontiguousarray(state_g, dtype=np.int32)
         a = self._any
+        if compact or isinstance(lines, LineList):
+            ll = lines if isinstance(lines, LineList) else LineList(
+                lines["nu"], lines["elow"], lines["aif"], lines["gns"], lines.get("gamma"),
+                lines.get("n"), compact=True)
+            cl = ll.c_lines()
+            check(lib().gexs_server_add_lines(self.h, C.byref(cl), a(se), a(sg), len(se),
+                                              float(mass), C.byref(lid)), "gexs_server_add_lines")
+            return lid.value
         check(lib().gexs_server_add_list(
             self.h, a(lines["nu"]), a(lines["elow"]), a(lines["aif"]), a(lines["gns"]),
             a(lines.get("gamma")), a(lines.get("n")), int(lines["nu"].shape[0]), a(se), a(sg),

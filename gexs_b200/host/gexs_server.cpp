@@ -49,8 +49,9 @@ constexpr int kQPoints = 4096;
 constexpr double kQTmin = 10.0, kQTmax = 10000.0;
 
 struct List {
-    double *nu = nullptr, *elow = nullptr, *aif = nullptr, *gamma = nullptr, *n = nullptr;
-    int32_t* gns = nullptr;
+    /* device copy of the list, in the format it was added in (FP64, or
+     * the 24-byte compact layout); the server owns every array */
+    gexs_lines lines{};
     int64_t count = 0;
     double* se = nullptr;
     int32_t* sg = nullptr;
@@ -60,6 +61,16 @@ struct List {
     double* d_qtab = nullptr;          /* Q at the table temperatures (HBM)   */
     std::vector<double> lnq;           /* ln Q, host mirror for job setup     */
 };
+
+void free_list(List& L)
+{
+    cudaFree(const_cast<double*>(L.lines.nu)); cudaFree(const_cast<double*>(L.lines.elow));
+    cudaFree(const_cast<double*>(L.lines.aif)); cudaFree(const_cast<int32_t*>(L.lines.gns));
+    cudaFree(const_cast<double*>(L.lines.gamma)); cudaFree(const_cast<double*>(L.lines.n));
+    cudaFree(L.se); cudaFree(L.sg); cudaFree(L.d_qtab);
+    L.lines = gexs_lines{};
+    L.se = nullptr; L.sg = nullptr; L.d_qtab = nullptr;
+}
 
 double qtab_lnt(int k)
 {
@@ -240,8 +251,7 @@ void launch_group(gexs_server* s, std::vector<Req*>& adm)
             j.precision = r->r.precision;
             j.quad_nodes = r->r.quad_nodes;
             j.accumulate = 0;
-            j.lines.nu = L.nu; j.lines.elow = L.elow; j.lines.aif = L.aif; j.lines.gns = L.gns;
-            j.lines.gamma = L.gamma; j.lines.n = L.n; j.lines.count = L.count;
+            j.lines = L.lines;
             void* d = nullptr;
             if (gexs::pool_alloc(gexs::ctx_pool(s->ctx), &d, output_bytes(r->r), st) != cudaSuccess) {
                 status = GEXS_ERR_OOM;
@@ -458,8 +468,7 @@ int gexs_server_destroy(gexs_server* s)
     /* every batch event still referenced, running or finished unfetched */
     for (auto& kv : s->ev_refs) cudaEventDestroy(kv.first);
     for (List& L : s->lists) {
-        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
-        cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.se); cudaFree(L.sg); cudaFree(L.d_qtab);
+        free_list(L);
     }
     for (cudaStream_t c : s->streams) cudaStreamDestroy(c);
     for (cudaStream_t c : s->copy_free) cudaStreamDestroy(c);
@@ -477,12 +486,30 @@ int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow, c
                          const double* state_energy, const int32_t* state_g, int64_t nstates,
                          double mean_mass, int* list_id)
 {
-    if (!s || !list_id || count < 0 || nstates <= 0 || !state_energy || !state_g ||
-        (count > 0 && (!nu || !elow || !aif || !gns)) || !(mean_mass > 0.0))
-        return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_add_list: arguments");
-    const bool press = gamma && n;
-    size_t bytes = (size_t)count * (3 * sizeof(double) + sizeof(int32_t) + (press ? 2 * sizeof(double) : 0)) +
-                   (size_t)nstates * (sizeof(double) + sizeof(int32_t)) + kQPoints * sizeof(double);
+    gexs_lines in;
+    std::memset(&in, 0, sizeof(in));
+    in.nu = nu; in.elow = elow; in.aif = aif; in.gns = gns; in.gamma = gamma; in.n = n;
+    in.count = count;
+    in.format = GEXS_LINES_FP64;
+    return gexs_server_add_lines(s, &in, state_energy, state_g, nstates, mean_mass, list_id);
+}
+
+int gexs_server_add_lines(gexs_server* s, const gexs_lines* in, const double* state_energy,
+                          const int32_t* state_g, int64_t nstates, double mean_mass, int* list_id)
+{
+    if (!s || !in || !list_id || in->count < 0 || nstates <= 0 || !state_energy || !state_g ||
+        !(mean_mass > 0.0) || (in->format != GEXS_LINES_FP64 && in->format != GEXS_LINES_COMPACT))
+        return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_add_lines: arguments");
+    const bool compact = in->format == GEXS_LINES_COMPACT;
+    const int64_t count = in->count;
+    if (count > 0 && (!in->nu || !in->elow || !in->aif || (!compact && !in->gns)))
+        return gexs::set_error(GEXS_ERR_INVALID, "gexs_server_add_lines: arrays");
+    const bool press = in->gamma && in->n;
+    /* bytes per line of each 4-or-8-byte field */
+    const size_t w = compact ? sizeof(float) : sizeof(double);
+    const size_t per_line = sizeof(double) + 2 * w + (compact ? 0 : sizeof(int32_t)) + (press ? 2 * w : 0);
+    const size_t bytes = (size_t)count * per_line + (size_t)nstates * (sizeof(double) + sizeof(int32_t)) +
+                         kQPoints * sizeof(double);
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (s->resident + s->inflight_bytes + bytes > s->budget)
@@ -491,47 +518,51 @@ int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow, c
     cudaSetDevice(s->device);
     List L;
     L.count = count; L.nstates = nstates; L.mass = mean_mass; L.bytes = bytes;
-    size_t c = (size_t)(count > 0 ? count : 1);
-    bool ok = cudaMalloc(&L.nu, sizeof(double) * c) == cudaSuccess &&
-              cudaMalloc(&L.elow, sizeof(double) * c) == cudaSuccess &&
-              cudaMalloc(&L.aif, sizeof(double) * c) == cudaSuccess &&
-              cudaMalloc(&L.gns, sizeof(int32_t) * c) == cudaSuccess &&
+    L.lines.count = count;
+    L.lines.format = in->format;
+    const size_t c = (size_t)(count > 0 ? count : 1);
+    void *d_nu = nullptr, *d_e = nullptr, *d_a = nullptr, *d_g = nullptr, *d_gam = nullptr, *d_n = nullptr;
+    bool ok = cudaMalloc(&d_nu, sizeof(double) * c) == cudaSuccess &&
+              cudaMalloc(&d_e, w * c) == cudaSuccess && cudaMalloc(&d_a, w * c) == cudaSuccess &&
+              (compact || cudaMalloc(&d_g, sizeof(int32_t) * c) == cudaSuccess) &&
+              (!press || (cudaMalloc(&d_gam, w * c) == cudaSuccess &&
+                          cudaMalloc(&d_n, w * c) == cudaSuccess)) &&
               cudaMalloc(&L.se, sizeof(double) * nstates) == cudaSuccess &&
-              cudaMalloc(&L.sg, sizeof(int32_t) * nstates) == cudaSuccess;
-    if (ok && press)
-        ok = cudaMalloc(&L.gamma, sizeof(double) * c) == cudaSuccess &&
-             cudaMalloc(&L.n, sizeof(double) * c) == cudaSuccess;
+              cudaMalloc(&L.sg, sizeof(int32_t) * nstates) == cudaSuccess &&
+              cudaMalloc(&L.d_qtab, sizeof(double) * kQPoints) == cudaSuccess;
+    L.lines.nu = (const double*)d_nu; L.lines.elow = (const double*)d_e; L.lines.aif = (const double*)d_a;
+    L.lines.gns = (const int32_t*)d_g; L.lines.gamma = (const double*)d_gam; L.lines.n = (const double*)d_n;
     if (!ok) {
-        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
-        cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n);
+        free_list(L);
         return gexs::set_error(GEXS_ERR_OOM, "line list upload");
     }
+    cudaError_t e = cudaSuccess;
+    auto put = [&](void* dst, const void* src, size_t n) {
+        if (e == cudaSuccess && n) e = cudaMemcpy(dst, src, n, cudaMemcpyDefault);
+    };
     if (count > 0) {
-        cudaMemcpy(L.nu, nu, sizeof(double) * count, cudaMemcpyDefault);
-        cudaMemcpy(L.elow, elow, sizeof(double) * count, cudaMemcpyDefault);
-        cudaMemcpy(L.aif, aif, sizeof(double) * count, cudaMemcpyDefault);
-        cudaMemcpy(L.gns, gns, sizeof(int32_t) * count, cudaMemcpyDefault);
+        put(d_nu, in->nu, sizeof(double) * count);
+        put(d_e, in->elow, w * count);
+        put(d_a, in->aif, w * count);
+        if (!compact) put(d_g, in->gns, sizeof(int32_t) * count);
         if (press) {
-            cudaMemcpy(L.gamma, gamma, sizeof(double) * count, cudaMemcpyDefault);
-            cudaMemcpy(L.n, n, sizeof(double) * count, cudaMemcpyDefault);
+            put(d_gam, in->gamma, w * count);
+            put(d_n, in->n, w * count);
         }
     }
-    cudaMemcpy(L.se, state_energy, sizeof(double) * nstates, cudaMemcpyDefault);
-    cudaError_t e = cudaMemcpy(L.sg, state_g, sizeof(int32_t) * nstates, cudaMemcpyDefault);
-    if (e != cudaSuccess) return gexs::cuda_error(e, "line list upload");
-    /* the resident Q(T) table */
-    if (cudaMalloc(&L.d_qtab, sizeof(double) * kQPoints) != cudaSuccess) {
-        cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
-        cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n);
-        return gexs::set_error(GEXS_ERR_OOM, "Q(T) table");
+    put(L.se, state_energy, sizeof(double) * nstates);
+    put(L.sg, state_g, sizeof(int32_t) * nstates);
+    if (e != cudaSuccess) {
+        free_list(L);
+        return gexs::cuda_error(e, "line list upload");
     }
+    /* the resident Q(T) table */
     {
         std::vector<double> temps(kQPoints), q;
         for (int k = 0; k < kQPoints; ++k) temps[k] = std::exp(qtab_lnt(k));
         const int st = exact_partitions(s, L, temps, q, L.d_qtab);
         if (st) {
-            cudaFree(L.nu); cudaFree(L.elow); cudaFree(L.aif); cudaFree(L.gns);
-            cudaFree(L.se); cudaFree(L.sg); cudaFree(L.gamma); cudaFree(L.n); cudaFree(L.d_qtab);
+            free_list(L);
             return st;
         }
         L.lnq.resize(kQPoints);
@@ -572,9 +603,7 @@ int gexs_server_submit(gexs_server* s, const gexs_request* r, uint64_t* ticket)
                 return gexs::set_error(GEXS_ERR_INVALID, "unknown list_id");
             }
             const List& L = s->lists[r->list_id];
-            probe.lines.nu = L.nu; probe.lines.elow = L.elow; probe.lines.aif = L.aif;
-            probe.lines.gns = L.gns; probe.lines.gamma = L.gamma; probe.lines.n = L.n;
-            probe.lines.count = L.count;
+            probe.lines = L.lines;
         }
         bool press = r->profile == GEXS_VOIGT || r->profile == GEXS_VOIGT_QUAD;
         if (press && !probe.lines.gamma) {

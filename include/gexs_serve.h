@@ -84,6 +84,15 @@ int gexs_server_add_list(gexs_server* s, const double* nu, const double* elow,
                          const int32_t* state_g, int64_t nstates, double mean_mass,
                          int* list_id);
 
+/* The same for a list described by a gexs_lines (host or device arrays),
+ * kept resident in the format it comes in: GEXS_LINES_FP64 (44 bytes per
+ * line with broadening) or GEXS_LINES_COMPACT (FP64 nu, float E'', g'A,
+ * gamma and n: 24 bytes per line; requests on it compute with the widened
+ * values, as gexs_run does). */
+int gexs_server_add_lines(gexs_server* s, const gexs_lines* lines, const double* state_energy,
+                          const int32_t* state_g, int64_t nstates, double mean_mass,
+                          int* list_id);
+
 /* Queue a request; returns at once with a ticket.  GEXS_ERR_ADMISSION if
  * the request alone can never fit in the budget. */
 int gexs_server_submit(gexs_server* s, const gexs_request* r, uint64_t* ticket);

@@ -109,6 +109,45 @@ def test_served_results_match_oracle(served, small_states, small_lines):
             assert rel <= H.FP32_REL and band <= H.FP32_BAND
 
 
+def test_compact_resident_list(small_states, small_lines):
+    """A list kept resident in the 24-byte compact layout: served results
+    equal gexs_run on the same compact list bit for bit, and the oracle on
+    the widened values within the stated tolerances."""
+    from oracle import pyoracle as po
+    from gexs_b200.engine import Context, Job, LineList
+    import torch
+    srv = Server(0, hbm_budget=1 << 30, streams=2)
+    try:
+        lid = srv.add_list(small_lines, small_states.energy, small_states.g, 18.0, compact=True)
+        ll = LineList(small_lines["nu"], small_lines["elow"], small_lines["aif"],
+                      small_lines["gns"], small_lines["gamma"], small_lines["n"], compact=True)
+        wide = ll.widened()
+        ctx = Context(0)
+        T, P, nu0, d, G = 900.0, 0.3, 500.0, 0.02, 50000
+        for prec in (capi.FP32, capi.FP64):
+            r = Server.request(lid, capi.VOIGT, T, P, nu0, d, G, precision=prec, cutoff=25.0)
+            out, _ = srv.wait(srv.submit(r), G)
+            q, _ = srv.partition(lid, T)
+            direct = torch.zeros(G, dtype=torch.float64, device="cuda")
+            j = Job(ll, direct, convention=capi.CONV_PHYSICAL, profile=capi.VOIGT, temperature=T,
+                    pressure=P, partition=q, mass=18.0, nu_start=nu0, dnu=d, grid_points=G,
+                    precision=prec, cutoff=25.0)
+            ctx.run([j])
+            ctx.check()
+            np.testing.assert_array_equal(out, direct.cpu().numpy())
+            jo = job_init(capi.CONV_PHYSICAL, capi.VOIGT, T, P,
+                          po.partition(small_states.energy, small_states.g, T), 18.0, nu0, d, G,
+                          cutoff=25.0)
+            ref = H.oracle_of(jo, wide)
+            if prec == capi.FP64:
+                assert np.all(np.abs(out - ref) <= 1e-10 * np.abs(ref))
+            else:
+                rel, band = H.fp32_errors(out, ref)
+                assert rel <= H.FP32_REL and band <= H.FP32_BAND
+    finally:
+        srv.close()
+
+
 def test_admission_by_budget(small_states, small_lines):
     line_bytes = sum(v.nbytes for v in small_lines.values()) + small_states.energy.nbytes * 2
     G = 200000
