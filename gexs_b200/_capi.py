@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(_HERE, "libgexs_b200.so")
 
 GEXS_OK = 0
 GEXS_ERR_INVALID = -1
+GEXS_ERR_OOM = -2
 GEXS_ERR_TIMEOUT = -4
 GEXS_ERR_NOT_READY = -5
 GEXS_ERR_ADMISSION = -6
@@ -167,6 +168,7 @@ SIGNATURES = [
     ("gexs_server_destroy", C.c_int, [C.c_void_p]),
     ("gexs_server_add_list", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 +
      [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int)]),
+    ("gexs_debug_fail_allocs", C.c_int, [C.c_int]),
     ("gexs_server_add_lines", C.c_int, [C.c_void_p, C.POINTER(GexsLines), C.c_void_p, C.c_void_p,
                                         C.c_int64, C.c_double, C.POINTER(C.c_int)]),
     ("gexs_server_submit", C.c_int, [C.c_void_p, C.POINTER(GexsRequest), C.POINTER(C.c_uint64)]),

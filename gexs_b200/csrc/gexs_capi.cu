@@ -8,6 +8,7 @@
  * returns a status and leaves a message for gexs_last_error().
  */
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -87,8 +88,14 @@ int ctx_device(gexs_ctx* c) { return c->device; }
 int ctx_sm_count(gexs_ctx* c) { return c->nsm; }
 cudaMemPool_t ctx_pool(gexs_ctx* c) { return c->pool; }
 
+/* gexs_debug_fail_allocs: allocations still to refuse (host-side fault
+ * injection for the out-of-memory paths; nothing reaches the device) */
+static std::atomic<int> g_fail_allocs{0};
+
 cudaError_t pool_alloc(cudaMemPool_t pool, void** p, size_t bytes, cudaStream_t s)
 {
+    for (int n = g_fail_allocs.load(); n > 0; n = g_fail_allocs.load())
+        if (g_fail_allocs.compare_exchange_weak(n, n - 1)) return cudaErrorMemoryAllocation;
     if (!pool) return cudaMallocAsync(p, bytes, s);
     cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
     if (e == cudaErrorMemoryAllocation) {
@@ -304,6 +311,13 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
 extern "C" {
 
 int gexs_version(void) { return 100; }
+
+int gexs_debug_fail_allocs(int n)
+{
+    if (n < 0) return set_error(GEXS_ERR_INVALID, "gexs_debug_fail_allocs: n < 0");
+    g_fail_allocs.store(n);
+    return GEXS_OK;
+}
 
 const char* gexs_status_string(int s)
 {

@@ -188,6 +188,11 @@ int         gexs_ctx_destroy(gexs_ctx* ctx);
 const char* gexs_status_string(int status);
 const char* gexs_last_error(void);
 int         gexs_version(void);
+/* Testing: refuse the next n stream-ordered device allocations of the
+ * library (launch scratch, server outputs) with an out-of-memory status,
+ * without calling CUDA, so that callers' out-of-memory paths can be
+ * exercised with no real memory pressure; 0 turns it off. */
+int         gexs_debug_fail_allocs(int n);
 
 /* Run njobs jobs (host array of descriptors holding device pointers) on
  * `stream`: one persistent launch over every (job, tile) work item.

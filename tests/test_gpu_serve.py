@@ -1,6 +1,7 @@
 """Request loop: admission by HBM budget, continuous batching, results
 identical alone and in a mix, failures reported per request."""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -145,6 +146,43 @@ def test_compact_resident_list(small_states, small_lines):
                 rel, band = H.fp32_errors(out, ref)
                 assert rel <= H.FP32_REL and band <= H.FP32_BAND
     finally:
+        srv.close()
+
+
+def test_out_of_memory_requeue_and_failure(small_states):
+    """Host-side fault injection (gexs_debug_fail_allocs refuses the next
+    allocation without calling CUDA): with nothing else running, the request
+    fails with GEXS_ERR_OOM and the server keeps serving; while another
+    batch runs, the group goes back to the queue and completes after that
+    batch with the same result as alone."""
+    from gexs_b200 import synth
+    from gexs_b200._capi import lib
+    L = synth.make_lines(small_states, 400000, 100.0, 4000.0, 2101, broadening_seed=3101)
+    srv = Server(0, hbm_budget=8 << 30, streams=2)
+    try:
+        lid = srv.add_list(L, small_states.energy, small_states.g, 18.0)
+        small = Server.request(lid, capi.VOIGT, 700.0, 0.5, 1000.0, 0.02, 20000,
+                               precision=capi.FP32, cutoff=25.0)
+        alone = srv.wait(srv.submit(small), 20000)[0]
+        assert lib().gexs_debug_fail_allocs(1) == 0
+        assert srv.wait_status(srv.submit(small), -1) == capi.GEXS_ERR_OOM
+        np.testing.assert_array_equal(srv.wait(srv.submit(small), 20000)[0], alone)
+        # a slow FP64 Gauss-Hermite batch holds the device meanwhile
+        big = Server.request(lid, capi.VOIGT_QUAD, 700.0, 0.5, 100.0, 0.01, 390001,
+                             precision=capi.FP64, cutoff=25.0, quad_nodes=32)
+        b0 = srv.stats()["batches"]
+        tb = srv.submit(big)
+        deadline = time.time() + 60
+        while srv.stats()["batches"] == b0 and time.time() < deadline:
+            time.sleep(0.0005)
+        assert lib().gexs_debug_fail_allocs(1) == 0
+        ts = srv.submit(small)
+        out, _ = srv.wait(ts, 20000)
+        assert srv.poll(tb) in (capi.GEXS_OK, capi.GEXS_ERR_NOT_READY)
+        srv.wait(tb, 390001)
+        np.testing.assert_array_equal(out, alone)
+    finally:
+        lib().gexs_debug_fail_allocs(0)
         srv.close()
 
 
