@@ -428,7 +428,8 @@ def batch64(ctx, torch, dev):
             "fp32_batched_ms": min(t32), "fp64_plain_ms": t64, "speedup": t64 / min(t32),
             "fp32_evals_per_s": evals / (min(t32) * 1e-3),
             "max_rel_err_vs_fp64": worst, "max_band_err_vs_fp64": band,
-            "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]},
+            "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1],
+                           "long_stages": bool(len(cfg) > 3 and cfg[3] & capi.LAUNCH_LONG_STAGES)},
             "grids": {"0.1": int(np.sum(dnus == 0.1)), "0.01": int(np.sum(dnus == 0.01)),
                       "0.005": int(np.sum(dnus == 0.005))}}
 
@@ -455,6 +456,9 @@ def batch_north_star(ctx, torch, dev, lines, st, fpe, fp64_peak, cfg):
                temperature=float(temps[i // 8]), pressure=float(press[i % 8]),
                partition=float(qs[i]), **kw) for i in range(64)]
     evals = sum(ctx.count_evals(j32))
+    # lines derived on load load the producers more: the 4-stage ring of
+    # 128-line stages serves this batch better (13.00 s against 13.16 s with
+    # 256-line stages, measured on one B200)
     bcfg = tuple(cfg[:3]) + (capi.LAUNCH_DERIVE_ON_LOAD,) + tuple(cfg[4:])
     b = ctx.batch(j32, bcfg)
     s = torch.cuda.Stream(device=dev)
@@ -938,7 +942,9 @@ def our_arm(args):
                        "parallelism": "replicas x%d" % ws if args.shard != "grid" else
                                       "grid-slices x%d" % ws,
                        "l2": "inputs (%.1f GB of lines) larger than L2" % (line_bytes / 1e9),
-                       "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1]}},
+                       "launch_cfg": {"bins_per_lane": cfg[0], "warps": cfg[1],
+                                      "long_stages": bool(len(cfg) > 3 and
+                                                          cfg[3] & capi.LAUNCH_LONG_STAGES)}},
             # per step: put_blob_kernel (launch table), prep_kernel (S(T),
             # width, y per line), slice_plan_kernel and slice_scan_kernel
             # (line slices), voigt_ws_kernel (region I), zero_ints_kernel
@@ -1031,8 +1037,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.3, 0.6, 0.9, 1.2])
     ap.add_argument("--autotune", action="store_true")
-    ap.add_argument("--cfg", default="4,4,0",
-                    help="launch shape bins_per_lane,warps,ctas_per_sm of the timed kernel")
+    ap.add_argument("--cfg", default="4,4,0,2",
+                    help="launch shape bins_per_lane,warps,ctas_per_sm[,flags] of the timed kernel")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     if args.warmup < 3:

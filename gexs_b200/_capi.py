@@ -53,6 +53,7 @@ class GexsLaunchCfg(C.Structure):
                 ("ctas_per_sm", C.c_int32), ("flags", C.c_int32), ("wait_spins", C.c_int32)]
 
 LAUNCH_DERIVE_ON_LOAD = 1
+LAUNCH_LONG_STAGES = 2
 
 
 class GexsRequest(C.Structure):

@@ -109,17 +109,19 @@ cudaError_t pool_alloc(cudaMemPool_t pool, void** p, size_t bytes, cudaStream_t 
 }
 }  // namespace gexs
 
+/* profile_class() of GEXS_VOIGT */
+constexpr int PK_VOIGT_CLASS = 0;
+
 static gexs_launch_cfg default_cfg(int pk, int prec)
 {
     /* measured best on B200 for the 1e8-line Voigt workload (FP32: 4 bins x
-     * 4 warps, FP64: 4 x 8); gexs_autotune replaces it per (profile,
-     * precision) */
+     * 4 warps with 256-line stages, FP64: 4 x 8); gexs_autotune replaces it
+     * per (profile, precision) */
     gexs_launch_cfg c{};
     c.bins_per_lane = 4;
     c.warps = (prec == GEXS_FP64) ? 8 : 4;
     c.ctas_per_sm = 0;
-    c.flags = 0;
-    (void)pk;
+    c.flags = (pk == PK_VOIGT_CLASS && prec == GEXS_FP32) ? GEXS_LAUNCH_LONG_STAGES : 0;
     return c;
 }
 
@@ -128,7 +130,8 @@ static bool cfg_ok(const gexs_launch_cfg& c, int prec)
     /* 16 bins per lane only for the FP32 form */
     return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8 ||
             (c.bins_per_lane == 16 && prec == GEXS_FP32)) &&
-           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0;
+           (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0 &&
+           (c.flags & ~(GEXS_LAUNCH_DERIVE_ON_LOAD | GEXS_LAUNCH_LONG_STAGES)) == 0;
 }
 
 static gexs_launch_cfg ctx_cfg(gexs_ctx* ctx, int pk, int prec)
@@ -687,10 +690,15 @@ int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs, gexs_launch_cf
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     float best_ms = 1e30f; gexs_launch_cfg bc = default_cfg(pk, prec);
     int st = GEXS_OK;
+    /* stage length is a further candidate where it exists (FP32 Voigt,
+     * 512-bin tiles) */
+    const bool stages = jobs[0].profile == GEXS_VOIGT && prec == GEXS_FP32;
     for (int bi = 0; bi < nbins && !st; ++bi)
-        for (int wi = 0; wi < 2 && !st; ++wi) {
+        for (int wi = 0; wi < 2 && !st; ++wi)
+        for (int li = 0; li < 2 && !st; ++li) {
+            if (li && !(stages && bins[bi] * warps[wi] == 16)) continue;
             gexs_launch_cfg c{}; c.bins_per_lane = bins[bi]; c.warps = warps[wi];
-            c.ctas_per_sm = 0; c.flags = 0;
+            c.ctas_per_sm = 0; c.flags = li ? GEXS_LAUNCH_LONG_STAGES : 0;
             gexs_batch* b = nullptr;
             st = gexs_batch_create(ctx, tj.data(), njobs, &c, &b);
             if (st) break;

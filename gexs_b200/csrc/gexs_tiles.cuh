@@ -1142,8 +1142,7 @@ tile_kernel(const KArgs args)
  *    bins-split form of the 4 x 4 shape (229 against 348 ms for 2 x 8).
  * Either way a bin's sum depends only on its tile's records, so results
  * are bitwise independent of batching. */
-constexpr int WS_STAGES = 4;
-constexpr int WS_R = 128;
+constexpr int WS_RING = 512;             /* records in the ring: stages x records per stage */
 constexpr int WS_SPIN = 1 << 21;          /* default try_wait attempts before giving up */
 
 struct StageHdr {
@@ -1188,8 +1187,9 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
     return false;
 }
 
-template <int B, int CONS, int PROD, bool PREP>
+template <int B, int CONS, int PROD, bool PREP, int SR>
 struct WsSmem {
+    static constexpr int WS_R = SR, WS_STAGES = WS_RING / SR;
     static constexpr int NP = PROD * 32;
     static constexpr int W = 32 * B * CONS;
     static constexpr int NF64 = PREP ? 4 : 5;
@@ -1207,11 +1207,12 @@ struct WsSmem {
     static constexpr size_t bytes = off_kahan + (size_t)(RS ? CONS : 1) * 2 * W * sizeof(float);
 };
 
-template <int B, int CONS, int PROD, bool PREP>
+template <int B, int CONS, int PROD, bool PREP, int SR>
 __global__ void __launch_bounds__((CONS + PROD) * 32, CONS == 4 ? (B >= 8 ? 3 : 4) : 2)
 voigt_ws_kernel(const KArgs args)
 {
-    typedef WsSmem<B, CONS, PROD, PREP> L;
+    typedef WsSmem<B, CONS, PROD, PREP, SR> L;
+    constexpr int WS_R = SR, WS_STAGES = WS_RING / SR;
     constexpr int NP = L::NP, W = L::W;
     constexpr int SUB = WS_R / NP;               /* lines per producer thread per stage */
     static_assert(WS_R % NP == 0, "stage size must be a multiple of the producer threads");
@@ -1813,12 +1814,12 @@ static cudaError_t launch_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStre
     return cudaGetLastError();
 }
 
-template <int B, int CONS, bool PREP>
-static cudaError_t launch_ws_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st)
+template <int B, int CONS, bool PREP, int SR>
+static cudaError_t launch_ws_sr(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st)
 {
     constexpr int PROD = 2;
-    auto kern = voigt_ws_kernel<B, CONS, PROD, PREP>;
-    const size_t smem = WsSmem<B, CONS, PROD, PREP>::bytes;
+    auto kern = voigt_ws_kernel<B, CONS, PROD, PREP, SR>;
+    const size_t smem = WsSmem<B, CONS, PROD, PREP, SR>::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
@@ -1832,23 +1833,37 @@ static cudaError_t launch_ws_one(const KArgs& a, int ctas_per_sm, int nsm, cudaS
     return cudaGetLastError();
 }
 
+/* records per ring stage: 128 (4 stages) by default; 256 (2 stages) on
+ * request (GEXS_LAUNCH_LONG_STAGES) for the record-split 512-bin shapes */
+template <int B, int CONS, bool PREP>
+static cudaError_t launch_ws_one(const KArgs& a, int ctas_per_sm, int nsm, cudaStream_t st,
+                                 bool long_stages)
+{
+    if constexpr (B * CONS == 16) {
+        if (long_stages) return launch_ws_sr<B, CONS, PREP, 256>(a, ctas_per_sm, nsm, st);
+    }
+    (void)long_stages;
+    return launch_ws_sr<B, CONS, PREP, 128>(a, ctas_per_sm, nsm, st);
+}
+
 /* FP32 Voigt: warp-specialised kernel, `warps` = consumer warps */
 template <bool PREP>
 static cudaError_t launch_ws(const KArgs& a, const gexs_launch_cfg& c, int nsm, cudaStream_t st)
 {
+    const bool ls = (c.flags & GEXS_LAUNCH_LONG_STAGES) != 0;
     if (c.warps == 4) {
         switch (c.bins_per_lane) {
-        case 2:  return launch_ws_one<2, 4, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 4:  return launch_ws_one<4, 4, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 8:  return launch_ws_one<8, 4, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 16: return launch_ws_one<16, 4, PREP>(a, c.ctas_per_sm, nsm, st);
+        case 2:  return launch_ws_one<2, 4, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 4:  return launch_ws_one<4, 4, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 8:  return launch_ws_one<8, 4, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 16: return launch_ws_one<16, 4, PREP>(a, c.ctas_per_sm, nsm, st, ls);
         }
     } else if (c.warps == 8) {
         switch (c.bins_per_lane) {
-        case 2:  return launch_ws_one<2, 8, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 4:  return launch_ws_one<4, 8, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 8:  return launch_ws_one<8, 8, PREP>(a, c.ctas_per_sm, nsm, st);
-        case 16: return launch_ws_one<16, 8, PREP>(a, c.ctas_per_sm, nsm, st);
+        case 2:  return launch_ws_one<2, 8, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 4:  return launch_ws_one<4, 8, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 8:  return launch_ws_one<8, 8, PREP>(a, c.ctas_per_sm, nsm, st, ls);
+        case 16: return launch_ws_one<16, 8, PREP>(a, c.ctas_per_sm, nsm, st, ls);
         }
     }
     return cudaErrorInvalidValue;

@@ -207,7 +207,7 @@ class Context:
         ms = C.c_float()
         check(lib().gexs_autotune(self.h, arr, len(arr), C.byref(best), C.byref(ms)),
               "gexs_autotune")
-        return (best.bins_per_lane, best.warps, best.ctas_per_sm), float(ms.value)
+        return (best.bins_per_lane, best.warps, best.ctas_per_sm, best.flags), float(ms.value)
 
     def partition(self, energy, g, temps):
         temps = np.ascontiguousarray(temps, dtype=np.float64)

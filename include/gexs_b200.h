@@ -176,6 +176,11 @@ typedef struct gexs_launch_cfg {
 /* derive S(T), width and y of every line in the tile loader instead of
  * once per job by a prep kernel (no per-job scratch of 24 B per line) */
 #define GEXS_LAUNCH_DERIVE_ON_LOAD 1
+/* FP32 Voigt, 512-bin tiles (4 bins x 4 warps, 2 x 8): hand lines from the
+ * producer warps to the consumers in stages of 256 instead of 128 (two
+ * stages in the ring instead of four).  Fewer hand-overs and Kahan folds,
+ * less slack between producers and consumers; gexs_autotune tries both. */
+#define GEXS_LAUNCH_LONG_STAGES    2
 
 /* A context owns a stream-ordered memory pool on its device for the
  * launch tables and per-line prep arrays (24 B per line) of gexs_run.  The
