@@ -8,15 +8,40 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace {
-const int kCopyChunks = 32;                     /* pieces of an overlapped line copy */
-const int kSegments = 5;                        /* grid segments of the first launch  */
-const double kSegmentFrac[kSegments] = {1.0 / 32, 1.0 / 8, 1.0 / 4, 1.0 / 2, 1.0};
+const int kCopyChunks = 64;                     /* pieces of an overlapped line copy */
+const int kSegments = 6;                        /* grid segments of the first launch  */
+const double kSegmentFrac[kSegments] = {1.0 / 64, 1.0 / 32, 1.0 / 8, 1.0 / 4, 1.0 / 2, 1.0};
 const int64_t kSegmentAlign = 4096;             /* widest tile: 32 lanes x 16 bins x 8 warps */
 const size_t kSegmentMinLines = (size_t)1 << 21;
 const size_t kSamples = 8192;
+
+/* memcpy of a grid-sized host array (tens of MB), split over up to 8
+ * threads; serial when a thread cannot be started */
+void par_copy(void* dst, const void* src, size_t bytes)
+{
+    const size_t kPart = (size_t)4 << 20;
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min(std::min((size_t)8, hw), std::max((size_t)1, bytes / kPart));
+    const size_t per = (bytes + nt - 1) / nt;
+    auto part = [=](size_t t) {
+        const size_t o = t * per;
+        if (o < bytes) std::memcpy((char*)dst + o, (const char*)src + o, std::min(per, bytes - o));
+    };
+    std::vector<std::thread> th;
+    size_t t = 1;
+    try {
+        for (; t < nt; ++t) th.emplace_back(part, t);
+    } catch (...) {
+        for (; t < nt; ++t) part(t);
+    }
+    part(0);
+    for (std::thread& x : th) x.join();
+}
 }  // namespace
 
 B200Manager::B200Manager(ProfileType profile, int device, int convention, int precision,
@@ -118,7 +143,7 @@ void B200Manager::TransferFreq(double* h_freq, double* h_intens, int N)
     if (status_) return;
     if (N != npoints_ || !h_freq || !h_intens) { fail(GEXS_ERR_INVALID); return; }
     cudaSetDevice(device_);
-    std::memcpy(h_freq_.data(), h_freq, sizeof(double) * (size_t)N);
+    par_copy(h_freq_.data(), h_freq, sizeof(double) * (size_t)N);
     for (double* d : d_slots_)
         if (cudaMemcpyAsync(d, h_intens, sizeof(double) * (size_t)N, cudaMemcpyHostToDevice,
                             (cudaStream_t)stream_) != cudaSuccess) { fail(GEXS_ERR_CUDA); return; }
@@ -324,7 +349,7 @@ void B200Manager::TransferResults(double* h_freq, double* h_intens, int N, int I
     cudaSetDevice(device_);
     int st = gexs_ctx_check(ctx_, stream_);
     if (st) { fail(st); return; }
-    if (h_freq) std::memcpy(h_freq, h_freq_.data(), sizeof(double) * (size_t)N);
+    if (h_freq) par_copy(h_freq, h_freq_.data(), sizeof(double) * (size_t)N);
     if (cudaMemcpy(h_intens, d_slots_[I], sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost) != cudaSuccess)
         fail(GEXS_ERR_CUDA);
 }
