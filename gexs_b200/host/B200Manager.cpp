@@ -347,9 +347,10 @@ void B200Manager::TransferResults(double* h_freq, double* h_intens, int N, int I
     if (I < 0 || I >= (int)d_slots_.size() || N > npoints_ || N < 0) { fail(GEXS_ERR_INVALID); return; }
     if (flush()) return;
     cudaSetDevice(device_);
+    /* the grid is host data: copied while the queued launches run */
+    if (h_freq) par_copy(h_freq, h_freq_.data(), sizeof(double) * (size_t)N);
     int st = gexs_ctx_check(ctx_, stream_);
     if (st) { fail(st); return; }
-    if (h_freq) par_copy(h_freq, h_freq_.data(), sizeof(double) * (size_t)N);
     if (cudaMemcpy(h_intens, d_slots_[I], sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost) != cudaSuccess)
         fail(GEXS_ERR_CUDA);
 }
