@@ -717,6 +717,78 @@ def quad_suite(args):
     return {"lines": lines.count, "grid_points": G, "temperature": T, "rows": res}
 
 
+def order_suite(args):
+    """Work-item order of a batch: --order-pairs (T, P) pairs (T log-spaced
+    100-3000 K x P log-spaced 1e-5-100 bar) of the --lines list on the
+    2,990,001-bin grid, FP32 Voigt with lines derived on load, launched with
+    items tile-major (the default) and job-major (GEXS_LAUNCH_JOB_MAJOR).
+    Default: each order as a graph-captured batch, one warm replay and
+    --steps timed replays (CUDA events), and whether the grids are bitwise
+    equal.  --order-plain: two plain launches per order (tile, job, tile,
+    job) and nothing timed, for an ncu capture of the last two."""
+    import torch
+    from gexs_b200 import Context, Job, LineList, synth, _capi as capi
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    st = synth.make_states(200000, 80, 1002)
+    L = synth.make_lines_torch(st, args.lines, NU0, NU1, 2002, broadening_seed=3002, device=dev)
+    lines = LineList(L["nu"], L["elow"], L["aif"], L["gns"], L["gamma"], L["n"], device=dev)
+    ctx = Context(0)
+    n = args.order_pairs
+    k = next(d for d in range(int(np.sqrt(n)), 0, -1) if n % d == 0)
+    temps = np.logspace(np.log10(100.0), np.log10(3000.0), k)
+    press = np.logspace(-5.0, 2.0, n // k)
+    qs = ctx.partition(torch.as_tensor(st.energy, device=dev),
+                       torch.as_tensor(st.g, dtype=torch.int32, device=dev), np.repeat(temps, n // k))
+    G = grid_points()
+
+    def jobs():
+        return [Job(lines, torch.zeros(G, dtype=torch.float64, device=dev),
+                    convention=capi.CONV_PHYSICAL, profile=capi.VOIGT,
+                    temperature=float(temps[i // (n // k)]), pressure=float(press[i % (n // k)]),
+                    partition=float(qs[i]), mass=MASS, nu_start=NU0, dnu=DNU, grid_points=G,
+                    precision=capi.FP32, cutoff=CUT) for i in range(n)]
+
+    flags = capi.LAUNCH_DERIVE_ON_LOAD
+    orders = (("tile_major", (4, 4, 0, flags)), ("job_major", (4, 4, 0, flags | capi.LAUNCH_JOB_MAJOR)))
+    res = {"suite": "order", "pairs": n, "lines": args.lines, "grid_points": G,
+           "launch_cfg": [4, 4, 0, flags]}
+    if args.order_plain:
+        J = jobs()
+        for _ in range(2):
+            for _, c in orders:
+                ctx.run(J, cfg=c)
+        ctx.check()
+        torch.cuda.synchronize()
+        return res
+    first = None
+    for name, c in orders:
+        J = jobs()
+        b = ctx.batch(J, c)
+        s = torch.cuda.Stream(device=dev)
+        b.capture(s)
+        b.replay(s)
+        s.synchronize()
+        ctx.check(s)
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.replay(s)
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ctx.check(s)
+        b.close()
+        res[name + "_ms"] = ts
+        if first is None:
+            first = [j.out for j in J]
+        else:
+            res["bitwise_equal"] = all(torch.equal(x, j.out) for x, j in zip(first, J))
+        del J
+    return res
+
+
 def ingest_suite(args):
     """ExoMol ingest: seeded .states (2e5 states, J 0-80) and .trans (the
     --ingest-lines transitions, 30-7000 cm^-1) text in the ExoMol layout,
@@ -1025,9 +1097,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the reference legs (CPU sample, reference GPU kernel)")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest", "serve"],
+    ap.add_argument("--suite", default="main", choices=["main", "quad", "ingest", "serve", "order"],
                     help="quad: Gauss-Hermite 16/32 vs Humlicek on the 5e8-line list; "
-                         "ingest: ExoMol text parsed on the GPU vs the reference reader")
+                         "ingest: ExoMol text parsed on the GPU vs the reference reader; "
+                         "order: a batch in tile-major and job-major item order")
     ap.add_argument("--ingest-lines", type=int, default=20_000_000)
     ap.add_argument("--quad-lines", type=int, default=500_000_000)
     ap.add_argument("--shard", default="replica", choices=["replica", "grid"],
@@ -1040,6 +1113,10 @@ def main():
     ap.add_argument("--cfg", default="4,4,0,2",
                     help="launch shape bins_per_lane,warps,ctas_per_sm[,flags] of the timed kernel")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--order-pairs", type=int, default=64,
+                    help="order suite: (T, P) pairs of the batch")
+    ap.add_argument("--order-plain", action="store_true",
+                    help="order suite: plain launches only (for an ncu capture)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -1053,6 +1130,9 @@ def main():
         torch.cuda.set_device(0)
         r = serve_bench(torch, "cuda:0", 0, args)
         print(json.dumps({"suite": "serve", **r}), flush=True)
+        return 0
+    if args.suite == "order":
+        print(json.dumps(order_suite(args)), flush=True)
         return 0
     if args.suite == "quad":
         r = quad_suite(args)

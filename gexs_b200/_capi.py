@@ -54,6 +54,7 @@ class GexsLaunchCfg(C.Structure):
 
 LAUNCH_DERIVE_ON_LOAD = 1
 LAUNCH_LONG_STAGES = 2
+LAUNCH_JOB_MAJOR = 4
 
 
 class GexsRequest(C.Structure):

@@ -131,7 +131,8 @@ static bool cfg_ok(const gexs_launch_cfg& c, int prec)
     return (c.bins_per_lane == 2 || c.bins_per_lane == 4 || c.bins_per_lane == 8 ||
             (c.bins_per_lane == 16 && prec == GEXS_FP32)) &&
            (c.warps == 4 || c.warps == 8) && c.ctas_per_sm >= 0 && c.wait_spins >= 0 &&
-           (c.flags & ~(GEXS_LAUNCH_DERIVE_ON_LOAD | GEXS_LAUNCH_LONG_STAGES)) == 0;
+           (c.flags & ~(GEXS_LAUNCH_DERIVE_ON_LOAD | GEXS_LAUNCH_LONG_STAGES |
+                        GEXS_LAUNCH_JOB_MAJOR)) == 0;
 }
 
 static gexs_launch_cfg ctx_cfg(gexs_ctx* ctx, int pk, int prec)
@@ -146,8 +147,42 @@ struct Group {
     int pk, prec;
     std::vector<gexs_job> jobs;
     std::vector<int> prefix;
+    std::vector<int> order;   /* tile-major order tables, empty: job-major */
     int nitems = 0;
 };
+
+/* Tile-major item order of a group with several jobs (GEXS_LAUNCH_JOB_MAJOR
+ * unset): item rows t = 0, 1, ... each hold tile t of every job that has
+ * more than t tiles.  With the jobs ranked by tile count (descending,
+ * stable), the rows fall into segments s = 0..nj-1 in which the first
+ * nj - s ranked jobs are active:
+ *   F[s]  first item of segment s (F[nj] = item count)
+ *   R[s]  first tile row of segment s
+ *   P[k]  job of rank k
+ * laid out as F | R | P (3 nj + 1 ints); decoded by tile_job on the device. */
+static std::vector<int> tile_order(const Group& g)
+{
+    const int nj = (int)g.jobs.size();
+    std::vector<int> n(nj), perm(nj);
+    for (int i = 0; i < nj; ++i) { n[i] = g.prefix[i + 1] - g.prefix[i]; perm[i] = i; }
+    std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return n[x] > n[y]; });
+    std::vector<int> out(3 * (size_t)nj + 1);
+    int* F = out.data();
+    int* R = F + nj + 1;
+    int* P = R + nj;
+    long long f = 0;
+    for (int s = 0; s < nj; ++s) {
+        const int active = nj - s;
+        const int r0 = s == 0 ? 0 : n[perm[nj - s]];   /* rows of the job that dropped out */
+        const int r1 = n[perm[nj - s - 1]];            /* fewest tiles among the active */
+        F[s] = (int)f;
+        R[s] = r0;
+        f += (long long)active * (r1 - r0);
+    }
+    F[nj] = (int)f;
+    for (int k = 0; k < nj; ++k) P[k] = perm[k];
+    return out;
+}
 
 static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* cfg_in,
                         gexs_ctx* ctx, std::vector<Group>& groups,
@@ -178,6 +213,9 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
         g.nitems += (int)tiles;
         g.prefix.push_back(g.nitems);
     }
+    for (size_t k = 0; k < groups.size(); ++k)
+        if (groups[k].jobs.size() > 1 && !(cfgs[k].flags & GEXS_LAUNCH_JOB_MAJOR))
+            groups[k].order = tile_order(groups[k]);
     return GEXS_OK;
 }
 
@@ -207,7 +245,7 @@ static Layout group_layout(const Group& g, bool prep, const gexs_launch_cfg& cfg
     auto up = [](size_t a) { return (a + 255) & ~size_t(255); };
     size_t a = up(g.jobs.size() * sizeof(gexs_job));
     L.op = a;
-    a = up(a + g.prefix.size() * sizeof(int));
+    a = up(a + (g.prefix.size() + g.order.size()) * sizeof(int));
     L.oc = a;
     a += 256;
     L.opp = a;
@@ -251,6 +289,9 @@ static std::vector<unsigned char> group_image(const Group& g, const Layout& L, u
     std::vector<unsigned char> h(L.oprep, 0);
     std::memcpy(h.data(), g.jobs.data(), g.jobs.size() * sizeof(gexs_job));
     std::memcpy(h.data() + L.op, g.prefix.data(), g.prefix.size() * sizeof(int));
+    if (!g.order.empty())
+        std::memcpy(h.data() + L.op + g.prefix.size() * sizeof(int), g.order.data(),
+                    g.order.size() * sizeof(int));
     double** pp = reinterpret_cast<double**>(h.data() + L.opp);
     for (size_t i = 0; i < g.jobs.size(); ++i)
         pp[i] = prep ? reinterpret_cast<double*>(dev + L.job_prep[i]) : nullptr;
@@ -308,7 +349,8 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
     return launch_tiles(g.pk, g.prec, (const gexs_job*)d, (const int*)(d + L.op),
                         (int)g.jobs.size(), g.nitems, (int*)(d + L.oc), d_err,
                         prep ? pp : nullptr, cfg, nsm, s, L.sliced ? &sl : nullptr,
-                        L.csliced ? &csl : nullptr);
+                        L.csliced ? &csl : nullptr,
+                        g.order.empty() ? nullptr : (const int*)(d + L.op) + g.prefix.size());
 }
 
 extern "C" {

@@ -34,6 +34,9 @@ struct SliceTables {
 
 /* d_prep: device array of per-job prep arrays (S | invw | y, 3 N doubles
  * each, from launch_prep), or NULL to derive every line on load.
+ * d_order: tile-major order tables of a launch with several jobs (F | R | P,
+ * 3 njobs + 1 ints, see tile_order in gexs_capi.cu), or NULL for job-major
+ * items.
  * d_counter: a 256-byte block of work counters; the caller zeroes the
  * first int, the FP32 Voigt core kernel's counter (int 32) is zeroed here
  * (by zero_ints). */
@@ -41,7 +44,7 @@ cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
                          cudaStream_t st, const SliceTables* sl = nullptr,
-                         const SliceTables* csl = nullptr);
+                         const SliceTables* csl = nullptr, const int* d_order = nullptr);
 /* which groups are sliced (all); lines_per_slice for a group (grows only
  * when the partial rows of its split tiles could pass 1 GiB) and the bound
  * on those rows */

@@ -128,10 +128,12 @@ int profile_class(const gexs_job& j)
 cudaError_t launch_tiles(int pk, int prec, const gexs_job* d_jobs, const int* d_prefix,
                          int njobs, int nitems, int* d_counter, int* d_err,
                          double* const* d_prep, const gexs_launch_cfg& cfg, int nsm,
-                         cudaStream_t st, const SliceTables* sl, const SliceTables* csl)
+                         cudaStream_t st, const SliceTables* sl, const SliceTables* csl,
+                         const int* d_order)
 {
     KArgs a;
     a.jobs = d_jobs; a.prefix = d_prefix; a.njobs = njobs; a.nitems = nitems;
+    a.order = njobs > 1 ? d_order : nullptr;
     a.counter = d_counter; a.err = d_err; a.prep = d_prep;
     a.tile_w = tile_bins(cfg);
     a.spin = cfg.wait_spins > 0 ? cfg.wait_spins : WS_SPIN;
@@ -169,10 +171,10 @@ __global__ void slice_plan_kernel(const KArgs a)
     const int lane = threadIdx.x & 31;
     const int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ti >= a.nitems) return;
-    int jl = 0, jh = a.njobs;
-    while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
+    int tj = 0;
+    const int jl = tile_job(a, ti, &tj);
     const gexs_job& J = a.jobs[jl];
-    const int64_t j0 = J.start_idx + (int64_t)(ti - __ldg(a.prefix + jl)) * a.tile_w;
+    const int64_t j0 = J.start_idx + (int64_t)tj * a.tile_w;
     const int jn = (int)min((int64_t)a.tile_w, J.start_idx + J.n_points - j0);
     const double f0 = grid_f(J.nu_start, J.dnu, j0);
     const double fl = grid_f(J.nu_start, J.dnu, j0 + jn - 1);
@@ -197,10 +199,10 @@ __global__ void core_slice_plan_kernel(const KArgs a)
     const int lane = threadIdx.x & 31;
     const int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ti >= a.nitems) return;
-    int jl = 0, jh = a.njobs;
-    while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
+    int tj = 0;
+    const int jl = tile_job(a, ti, &tj);
     const gexs_job& J = a.jobs[jl];
-    const int64_t t0 = J.start_idx + (int64_t)(ti - __ldg(a.prefix + jl)) * a.tile_w;
+    const int64_t t0 = J.start_idx + (int64_t)tj * a.tile_w;
     const int64_t tend = min((int64_t)(t0 + a.tile_w), J.start_idx + J.n_points);
     const int jn = (int)min((int64_t)CORE_W, tend - t0);
     const double f0 = grid_f(J.nu_start, J.dnu, t0);

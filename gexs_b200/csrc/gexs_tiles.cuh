@@ -324,7 +324,33 @@ struct KArgs {
     SliceTables     sl;        /* line slices (sl.prefix NULL: none)     */
     SliceTables     csl;       /* FP32 Voigt core kernel's slices        */
     int             spin;      /* try_wait attempts of every bounded wait */
+    const int*      order;     /* tile-major order tables F|R|P, or NULL
+                                  for job-major items (gexs_capi.cu
+                                  tile_order)                           */
 };
+
+/* flat tile index ti (the index the slice tables use) -> job, and the
+ * tile of that job in *tile.  Job-major: the last job whose prefix is
+ * <= ti.  Tile-major: the segment s of ti (last F[s] <= ti) has its first
+ * nj - s ranked jobs active, one tile of each per row. */
+__device__ __forceinline__ int tile_job(const KArgs& a, int ti, int* tile)
+{
+    const int nj = a.njobs;
+    if (a.order) {
+        const int* F = a.order;
+        const int* R = F + nj + 1;
+        const int* P = R + nj;
+        int lo = 0, hi = nj;
+        while (hi - lo > 1) { int m = (lo + hi) >> 1; if (__ldg(F + m) <= ti) lo = m; else hi = m; }
+        const int act = nj - lo, d = ti - __ldg(F + lo);
+        *tile = __ldg(R + lo) + d / act;
+        return __ldg(P + d % act);
+    }
+    int jl = 0, jh = nj;
+    while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(a.prefix + m) <= ti) jl = m; else jh = m; }
+    *tile = ti - __ldg(a.prefix + jl);
+    return jl;
+}
 
 /* slice_plan_kernel + slice_scan_kernel (gexs_kernels.cu): every tile's
  * line range and slice count, then the item prefix and count */
@@ -751,18 +777,28 @@ __device__ __forceinline__ void voigt_rs_record(const RecV& r, int lane, float2 
     const int tiers = r.tiers;
     const float2 n0 = __fadd2_rn(r.nb, lw2);
     if (tiers == kAll) {
-        const float2 step = make_float2(64.f, 64.f);
         const float2 dx = r.dx, mf = r.mf, c = r.c, y2 = r.y2, a2 = r.a;
-        float2 n2 = n0;
+        /* n of pair j is n0 + 64 j, built as a tree: n_j = n_{j-2^h} +
+         * 64 * 2^h with 2^h the highest power of two in j.  The values are
+         * the exact small integers that stepping n += 64 gives, with a
+         * dependency depth of log2(pairs) instead of pairs - 1 (measured:
+         * 1.4 ms less per 1e8-line cross-section, the same sums). */
+        float2 nn[B * CONS / 2];
+        nn[0] = n0;
+#pragma unroll
+        for (int j = 1; j < B * CONS / 2; ++j) {
+            const int h = 31 - __clz(j);
+            const float sj = 64.f * (float)(1 << h);
+            nn[j] = __fadd2_rn(nn[j - (1 << h)], make_float2(sj, sj));
+        }
 #pragma unroll
         for (int j = 0; j < B * CONS / 2; ++j) {
-            const float2 x = __ffma2_rn(n2, dx, mf);
+            const float2 x = __ffma2_rn(nn[j], dx, mf);
             const float2 m = __ffma2_rn(x, x, c);
             const float2 d = __ffma2_rn(m, m, y2);
             float2 rr;
             rr.x = rcp_approx(d.x); rr.y = rcp_approx(d.y);
             part[j] = __ffma2_rn(__ffma2_rn(m, rr, rr), a2, part[j]);
-            n2 = __fadd2_rn(n2, step);
         }
         return;
     }
@@ -931,13 +967,13 @@ tile_kernel(const KArgs args)
         }
 
         /* job of this tile: last prefix entry <= tile */
-        int jl = 0, jh = args.njobs;
-        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
+        int tj = 0;
+        const int jl = tile_job(args, ti, &tj);
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
         Tile T;
         T.J = Jp;
-        T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * W;
+        T.j0 = J.start_idx + (int64_t)tj * W;
         T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
         T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
         T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
@@ -1276,13 +1312,13 @@ voigt_ws_kernel(const KArgs args)
                 sidx = item - __ldg(args.sl.prefix + tl);
                 ns = __ldg(args.sl.prefix + tl + 1) - __ldg(args.sl.prefix + tl);
             }
-            int jl = 0, jh = args.njobs;
-            while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
+            int tj = 0;
+            const int jl = tile_job(args, ti, &tj);
             const gexs_job* Jp = args.jobs + jl;
             const gexs_job& J = *Jp;
             Tile T;
             T.J = Jp;
-            T.j0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * W;
+            T.j0 = J.start_idx + (int64_t)tj * W;
             T.jn = (int)min((int64_t)W, J.start_idx + J.n_points - T.j0);
             T.f0 = grid_f(J.nu_start, J.dnu, T.j0);
             T.fl = grid_f(J.nu_start, J.dnu, T.j0 + T.jn - 1);
@@ -1635,12 +1671,12 @@ core_kernel(const KArgs args)
             sidx = item - __ldg(args.csl.prefix + tl);
             ns = __ldg(args.csl.prefix + tl + 1) - __ldg(args.csl.prefix + tl);
         }
-        int jl = 0, jh = args.njobs;
-        while (jh - jl > 1) { int m = (jl + jh) >> 1; if (__ldg(args.prefix + m) <= ti) jl = m; else jh = m; }
+        int tj = 0;
+        const int jl = tile_job(args, ti, &tj);
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
         /* the region-I kernel's tile of this item */
-        const int64_t t0 = J.start_idx + (int64_t)(ti - __ldg(args.prefix + jl)) * args.tile_w;
+        const int64_t t0 = J.start_idx + (int64_t)tj * args.tile_w;
         const int64_t tend = min((int64_t)(t0 + args.tile_w), J.start_idx + J.n_points);
         const int64_t nl = J.lines.count;
         const double* pb = PREP ? args.prep[jl] : nullptr;

@@ -181,6 +181,14 @@ typedef struct gexs_launch_cfg {
  * stages in the ring instead of four).  Fewer hand-overs and Kahan folds,
  * less slack between producers and consumers; gexs_autotune tries both. */
 #define GEXS_LAUNCH_LONG_STAGES    2
+/* Work-item order of a launch with several jobs.  By default the items go
+ * tile-major: tile 0 of every job, then tile 1 of every job, and so on
+ * (jobs with fewer tiles drop out as they end), so the jobs of a (T, P)
+ * batch over one line list read a tile's lines from HBM once and from L2
+ * for the other pairs while the CTAs that run them are resident together.
+ * This flag restores job-major order (all tiles of job 0, then job 1, ...).
+ * A tile's sums do not depend on the order: results are bitwise equal. */
+#define GEXS_LAUNCH_JOB_MAJOR      4
 
 /* A context owns a stream-ordered memory pool on its device for the
  * launch tables and per-line prep arrays (24 B per line) of gexs_run.  The
