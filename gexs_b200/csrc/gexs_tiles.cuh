@@ -333,10 +333,11 @@ struct KArgs {
  * tile of that job in *tile.  Job-major: the last job whose prefix is
  * <= ti.  Tile-major: the segment s of ti (last F[s] <= ti) has its first
  * nj - s ranked jobs active, one tile of each per row. */
+template <bool ORDER = true>
 __device__ __forceinline__ int tile_job(const KArgs& a, int ti, int* tile)
 {
     const int nj = a.njobs;
-    if (a.order) {
+    if (ORDER && a.order) {
         const int* F = a.order;
         const int* R = F + nj + 1;
         const int* P = R + nj;
@@ -1642,7 +1643,9 @@ __device__ __forceinline__ void core_ranges(int c1, int c2, int c3, int& c1a, in
     if (c3a >= c3b) c3a = c3b = c2b;
 }
 
-template <bool PREP>
+/* ORDER: the launch's items may be tile-major (its own instantiation: the
+ * decode's divisions cost this kernel 8 registers when compiled in) */
+template <bool PREP, bool ORDER>
 __global__ void __launch_bounds__(CORE_WARPS * 32)
 core_kernel(const KArgs args)
 {
@@ -1672,7 +1675,7 @@ core_kernel(const KArgs args)
             ns = __ldg(args.csl.prefix + tl + 1) - __ldg(args.csl.prefix + tl);
         }
         int tj = 0;
-        const int jl = tile_job(args, ti, &tj);
+        const int jl = tile_job<ORDER>(args, ti, &tj);
         const gexs_job* Jp = args.jobs + jl;
         const gexs_job& J = *Jp;
         /* the region-I kernel's tile of this item */
@@ -1944,7 +1947,7 @@ constexpr int CORE_COUNTER_OFFSET = 32;
 template <bool PREP>
 static cudaError_t launch_core(const KArgs& a, int nsm, cudaStream_t st)
 {
-    auto kern = core_kernel<PREP>;
+    auto kern = a.order ? core_kernel<PREP, true> : core_kernel<PREP, false>;
     const size_t smem = CoreSmem::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

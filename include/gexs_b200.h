@@ -187,7 +187,8 @@ typedef struct gexs_launch_cfg {
  * batch over one line list read a tile's lines from HBM once and from L2
  * for the other pairs while the CTAs that run them are resident together.
  * This flag restores job-major order (all tiles of job 0, then job 1, ...).
- * A tile's sums do not depend on the order: results are bitwise equal. */
+ * A tile's sums do not depend on the order: results are bitwise equal.
+ * gexs_autotune tries both for several jobs. */
 #define GEXS_LAUNCH_JOB_MAJOR      4
 
 /* A context owns a stream-ordered memory pool on its device for the
@@ -386,8 +387,11 @@ int gexs_batch_capture(gexs_batch* b, void* stream);  /* build the graph   */
 int gexs_batch_replay(gexs_batch* b, void* stream);   /* launch the graph  */
 int gexs_batch_destroy(gexs_batch* b);
 
-/* Pick bins_per_lane / warps / ctas_per_sm for these jobs by timing each
- * candidate (CUDA events) on the jobs themselves.  Writes the winner to
+/* Pick the launch for these jobs by timing each candidate (CUDA events) on
+ * the jobs themselves: bins_per_lane x warps (the tile width and CTA
+ * shape), the ring's stage length where it applies (GEXS_LAUNCH_LONG_STAGES)
+ * and, for several jobs, the item order on the best shape
+ * (GEXS_LAUNCH_JOB_MAJOR or the tile-major default).  Writes the winner to
  * *best and records it as the context default for the jobs' profile and
  * precision; h_ms (may be NULL) gets the winner's time. */
 int gexs_autotune(gexs_ctx* ctx, const gexs_job* jobs, int njobs,

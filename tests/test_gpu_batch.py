@@ -89,4 +89,15 @@ def test_autotune_returns_a_valid_shape(gpu_ctx, small_lines):
     lines = LineList.from_dict(small_lines)
     jobs = _pairs(lines, capi.FP32, n=3)
     cfg, ms = gpu_ctx.autotune(jobs)
-    assert cfg[0] in (2, 4, 8) and cfg[1] in (4, 8) and ms > 0
+    assert cfg[0] in (2, 4, 8, 16) and cfg[1] in (4, 8) and ms > 0
+    # flags: at most the stage length and, for several jobs, the item order
+    assert cfg[3] & ~(capi.LAUNCH_LONG_STAGES | capi.LAUNCH_JOB_MAJOR) == 0
+    # the tuned launch is the context default now: same bits as tile-major
+    a = _pairs(lines, capi.FP32, n=3)
+    b = _pairs(lines, capi.FP32, n=3)
+    gpu_ctx.run(a)
+    gpu_ctx.run(b, cfg=(4, 4, 0, capi.LAUNCH_LONG_STAGES))
+    gpu_ctx.check()
+    if cfg[:2] == (4, 4) and cfg[3] & capi.LAUNCH_LONG_STAGES:
+        for x, y in zip(a, b):
+            assert torch.equal(x.out, y.out)
