@@ -171,6 +171,7 @@ SIGNATURES = [
     ("gexs_server_add_list", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 +
      [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int)]),
     ("gexs_debug_fail_allocs", C.c_int, [C.c_int]),
+    ("gexs_debug_tile_order", C.c_int, [C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_int32)]),
     ("gexs_server_add_lines", C.c_int, [C.c_void_p, C.POINTER(GexsLines), C.c_void_p, C.c_void_p,
                                         C.c_int64, C.c_double, C.POINTER(C.c_int)]),
     ("gexs_server_submit", C.c_int, [C.c_void_p, C.POINTER(GexsRequest), C.POINTER(C.c_uint64)]),

@@ -160,11 +160,11 @@ struct Group {
  *   R[s]  first tile row of segment s
  *   P[k]  job of rank k
  * laid out as F | R | P (3 nj + 1 ints); decoded by tile_job on the device. */
-static std::vector<int> tile_order(const Group& g)
+static std::vector<int> tile_order(const std::vector<int>& n)
 {
-    const int nj = (int)g.jobs.size();
-    std::vector<int> n(nj), perm(nj);
-    for (int i = 0; i < nj; ++i) { n[i] = g.prefix[i + 1] - g.prefix[i]; perm[i] = i; }
+    const int nj = (int)n.size();
+    std::vector<int> perm(nj);
+    for (int i = 0; i < nj; ++i) perm[i] = i;
     std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return n[x] > n[y]; });
     std::vector<int> out(3 * (size_t)nj + 1);
     int* F = out.data();
@@ -215,7 +215,12 @@ static int build_groups(const gexs_job* jobs, int njobs, const gexs_launch_cfg* 
     }
     for (size_t k = 0; k < groups.size(); ++k)
         if (groups[k].jobs.size() > 1 && !(cfgs[k].flags & GEXS_LAUNCH_JOB_MAJOR))
-            groups[k].order = tile_order(groups[k]);
+        {
+            const Group& g = groups[k];
+            std::vector<int> n(g.jobs.size());
+            for (size_t i = 0; i < n.size(); ++i) n[i] = g.prefix[i + 1] - g.prefix[i];
+            groups[k].order = tile_order(n);
+        }
     return GEXS_OK;
 }
 
@@ -356,6 +361,21 @@ static cudaError_t enqueue_group(const Group& g, const Layout& L, unsigned char*
 extern "C" {
 
 int gexs_version(void) { return 100; }
+
+int gexs_debug_tile_order(const int32_t* tiles, int njobs, int32_t* out)
+{
+    if (!tiles || !out || njobs < 1) return set_error(GEXS_ERR_INVALID, "gexs_debug_tile_order: arguments");
+    std::vector<int> n(tiles, tiles + njobs);
+    long long total = 0;
+    for (int v : n) {
+        if (v < 0) return set_error(GEXS_ERR_INVALID, "gexs_debug_tile_order: negative tile count");
+        total += v;
+    }
+    if (total > (long long)INT32_MAX) return set_error(GEXS_ERR_INVALID, "gexs_debug_tile_order: too many tiles");
+    const std::vector<int> o = tile_order(n);
+    std::memcpy(out, o.data(), o.size() * sizeof(int32_t));
+    return GEXS_OK;
+}
 
 int gexs_debug_fail_allocs(int n)
 {

@@ -207,6 +207,13 @@ int         gexs_version(void);
  * without calling CUDA, so that callers' out-of-memory paths can be
  * exercised with no real memory pressure; 0 turns it off. */
 int         gexs_debug_fail_allocs(int n);
+/* Testing: the tile-major order tables a launch of njobs jobs with these
+ * tile counts uses (GEXS_LAUNCH_JOB_MAJOR unset), written to out
+ * (3 njobs + 1 ints: F[njobs + 1] first item of each segment, R[njobs]
+ * first tile row of each segment, P[njobs] job of each rank; in segment s
+ * the jobs P[0 .. njobs - s) are active, one tile of each per row).  Host
+ * only; no device work. */
+int         gexs_debug_tile_order(const int32_t* tiles, int njobs, int32_t* out);
 
 /* Run njobs jobs (host array of descriptors holding device pointers) on
  * `stream`: one persistent launch over every (job, tile) work item.
