@@ -434,7 +434,7 @@ def batch64(ctx, torch, dev):
                       "0.005": int(np.sum(dnus == 0.005))}}
 
 
-def batch_north_star(ctx, torch, dev, lines, st, fpe, fp64_peak, cfg):
+def batch_64_pairs_full_list(ctx, torch, dev, lines, st, fpe, fp64_peak, cfg):
     """64 (T, P) cross-sections of the 1e8-line list on the 2,990,001-bin grid
     (T log-spaced 100-3000 K x P log-spaced 1e-5-100 bar, 0.01 cm^-1 over
     100-30000, cutoff 25): the FP32 form as one batch (gexs_batch, lines
@@ -1065,7 +1065,7 @@ def our_arm(args):
         log("64-pair batch on the 1e6-line list")
         result["batch64"] = batch64(ctx, torch, dev)
         log("64 pairs of the 1e8-line list")
-        result["batch_64_pairs_1e8_lines"] = batch_north_star(
+        result["batch_64_pairs_1e8_lines"] = batch_64_pairs_full_list(
             ctx, torch, dev, lines, st, result["roofline"]["flop_per_eval"],
             result["roofline"].get("fp64_peak_tflops"), cfg)
     if not args.no_serve and rank == 0:
