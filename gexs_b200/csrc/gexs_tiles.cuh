@@ -332,7 +332,8 @@ struct KArgs {
 /* flat tile index ti (the index the slice tables use) -> job, and the
  * tile of that job in *tile.  Job-major: the last job whose prefix is
  * <= ti.  Tile-major: the segment s of ti (last F[s] <= ti) has its first
- * nj - s ranked jobs active, one tile of each per row. */
+ * nj - s ranked jobs active, one tile of each per row.  ORDER = false
+ * compiles the job-major search alone (for builds that never see a.order). */
 template <bool ORDER = true>
 __device__ __forceinline__ int tile_job(const KArgs& a, int ti, int* tile)
 {
